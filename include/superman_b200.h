@@ -1,0 +1,125 @@
+/*
+ * superman_b200 — C ABI of the B200 (sm_100a) matrix-permanent library.
+ *
+ * This is the drop-in boundary for SUPerman's Ryser/Gray-code hot path.  Each
+ * entry point replaces one reference interface (cited per declaration, paths
+ * relative to the SUPerman source tree).  Plain pointers and sizes only; every
+ * call returns a status code instead of exiting (the reference's gpuErrchk
+ * calls exit(), Algorithms/GPU/GPUHelpers.cuh:77-85).
+ *
+ * Matrices are row-major, n x n, 1 <= n <= 63 (the reference's limit,
+ * CommonFiles/DecomposePerman.h:185-188 and Algorithms/GPU/GPUHelpers.cuh:38).
+ * Inputs are caller-owned host arrays unless the name ends in _dev.
+ */
+#ifndef SUPERMAN_B200_H
+#define SUPERMAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SPB_API __attribute__((visibility("default")))
+#else
+#define SPB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status ---- */
+enum spb_status {
+    SPB_OK = 0,
+    SPB_ERR_INVALID = 1,    /* bad argument: null pointer, n out of range      */
+    SPB_ERR_CUDA = 2,       /* a CUDA runtime call failed (see spb_last_error) */
+    SPB_ERR_NO_DEVICE = 3,  /* no usable CUDA device                           */
+    SPB_ERR_OOM = 4,        /* device or host allocation failed                */
+    SPB_ERR_OVERFLOW = 5,   /* exact integer result does not fit               */
+    SPB_ERR_TIMEOUT = 6,    /* a bounded wait ran out                          */
+    SPB_ERR_CANCELLED = 7,  /* the request was cancelled                       */
+    SPB_ERR_BUSY = 8,       /* admission refused: queue or scratch full        */
+    SPB_ERR_IO = 9,         /* file could not be opened or parsed              */
+    SPB_ERR_NOT_SQUARE = 10 /* matrix file header is not square                */
+};
+
+/* Precision modes.  SPB_PREC_FP64 corresponds to the reference's default
+ * `calculation_precision=kahan` (CommonFiles/Settings.h:59-65, IO/IO.h:178)
+ * and SPB_PREC_DD to `calculation_precision=dd`. */
+enum spb_precision {
+    SPB_PREC_FP64 = 0, /* FP64 row sums and products, double-double sum      */
+    SPB_PREC_DD = 1    /* + double-double re-evaluation of dominant units    */
+};
+
+typedef struct spb_options {
+    int device;            /* CUDA ordinal (Settings::deviceID)              */
+    int precision;         /* enum spb_precision                             */
+    double rel_tol;        /* SPB_PREC_DD target relative error (0 = 1e-13)  */
+    int unit_bits;         /* log2 Gray terms per unit; 0 = automatic        */
+    int threads_per_block; /* 0 = automatic                                  */
+    int blocks;            /* 0 = automatic (persistent: one CTA per SM)     */
+    void* stream;          /* cudaStream_t to run on; NULL = library stream  */
+} spb_options;
+
+typedef struct spb_result {
+    double value;          /* permanent (real part), rounded double-double  */
+    double value_lo;       /* low word of the double-double result          */
+    double imag;           /* imaginary part (complex entry points)         */
+    double imag_lo;
+    double elapsed_s;      /* wall time of the whole call                   */
+    double kernel_s;       /* device time of the Gray-walk kernels          */
+    double err_est;        /* estimated relative error (statistical)        */
+    uint64_t gray_steps;   /* Gray steps walked: n*2^(n-1) (NW) or n*2^n    */
+    uint64_t refined_units;/* units re-evaluated in double-double           */
+    int status;            /* enum spb_status                               */
+    int launches;          /* kernels launched by the call                  */
+} spb_result;
+
+/* Fills *opt with the defaults (device 0, SPB_PREC_FP64, automatic shape). */
+SPB_API void spb_default_options(spb_options* opt);
+
+/* Message of the last failed call on this host thread ("" if none). */
+SPB_API const char* spb_last_error(void);
+
+/* Static name of a status code. */
+SPB_API const char* spb_status_string(int status);
+
+/* Library version as major*10000 + minor*100 + patch. */
+SPB_API int spb_version(void);
+
+/* Number of CUDA devices visible (0 when none; never fails). */
+SPB_API int spb_device_count(void);
+
+/* Dense real permanent by the Nijenhuis–Wilf Ryser formula with Gray-code
+ * enumeration.  Replaces the dense single-GPU driver
+ * dpSingleGPU<C,S,Algo,Shared>::permanentFunction
+ * (Algorithms/GPU/Dense/dpSingleGPU.cuh:45-219) and its kernels
+ * xRegisterMShared[Kahan] (Algorithms/GPU/Dense/DenseKernelDefinitions.cuh:
+ * 189-264, 331-405).  a: n*n doubles, row-major. */
+SPB_API int spb_perm_dense_f64(const double* a, int n, const spb_options* opt, spb_result* out);
+
+/* Same on a device-resident row-major matrix. */
+SPB_API int spb_perm_dense_f64_dev(const double* d_a, int n, const spb_options* opt,
+                           spb_result* out);
+
+/* Dense complex128 permanent.  Replaces gpuComputeComplex
+ * (Algorithms/Complex/gpuComputeComplex.cu:199-418, declared in
+ * Algorithms/Complex/gpuComputeComplex.cuh:33) and its kernel
+ * xRegisterMSharedComplex (gpuComputeComplex.cu:39-117).
+ * a: n*n (re, im) pairs, row-major, 2*n*n doubles. */
+SPB_API int spb_perm_dense_c128(const double* a, int n, const spb_options* opt, spb_result* out);
+
+/* Same on a device-resident interleaved matrix. */
+SPB_API int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options* opt,
+                            spb_result* out);
+
+/* Measured pipe throughput used as the roofline denominator: which = 0 gives
+ * FP64 FMA thread-instructions per second, which = 1 gives int32 multiply-add
+ * thread-instructions per second (best of three timed launches).  No
+ * reference counterpart: the reference reports no roofline. */
+SPB_API int spb_measure_pipe_peak(int device, int which, double* ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUPERMAN_B200_H */

@@ -1,0 +1,81 @@
+"""superman_b200 — B200-native (sm_100a) exact matrix permanents.
+
+Python host mirror of SUPerman's permanent API over the C ABI in
+include/superman_b200.h.  The compute path is libsupb200.so (hand-written CUDA
+for sm_100a); there is no CPU fallback.
+
+    from superman_b200 import perm_dense, perm_complex
+    r = perm_dense(a)          # Result(time, permanent, ...)
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
+
+__all__ = ["Result", "perm_dense", "perm_complex", "SupermanError", "SPB_PREC_FP64",
+           "SPB_PREC_DD", "device_count"]
+
+_PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD}
+
+
+@dataclass
+class Result:
+    """Mirror of the reference's Result record {time, permanent}
+    (CommonFiles/Result.h:29-37) with the extra fields the C ABI reports."""
+    time: float
+    permanent: complex | float
+    permanent_lo: float = 0.0
+    imag_lo: float = 0.0
+    kernel_s: float = 0.0
+    err_est: float = 0.0
+    gray_steps: int = 0
+    refined_units: int = 0
+    launches: int = 0
+
+
+def device_count() -> int:
+    return _lib.lib().spb_device_count()
+
+
+def _options(precision, device, **shape):
+    p = _PREC[precision] if isinstance(precision, str) else int(precision)
+    return _lib.default_options(device=device, precision=p, **shape)
+
+
+def _to_result(r: _lib.spb_result, complex_: bool) -> Result:
+    val = complex(r.value, r.imag) if complex_ else r.value
+    return Result(time=r.elapsed_s, permanent=val, permanent_lo=r.value_lo, imag_lo=r.imag_lo,
+                  kernel_s=r.kernel_s, err_est=r.err_est, gray_steps=r.gray_steps,
+                  refined_units=r.refined_units, launches=r.launches)
+
+
+def perm_dense(a, precision="fp64", device: int = 0, **shape) -> Result:
+    """Permanent of a dense real n x n matrix (1 <= n <= 63)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("perm_dense needs a square 2-D array")
+    out = _lib.spb_result()
+    opt = _options(precision, device, **shape)
+    st = _lib.lib().spb_perm_dense_f64(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       a.shape[0], ctypes.byref(opt), ctypes.byref(out))
+    _lib.check(st)
+    return _to_result(out, False)
+
+
+def perm_complex(a, precision="fp64", device: int = 0, **shape) -> Result:
+    """Permanent of a dense complex128 n x n matrix (1 <= n <= 63)."""
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("perm_complex needs a square 2-D array")
+    out = _lib.spb_result()
+    opt = _options(precision, device, **shape)
+    ri = a.view(np.float64)
+    st = _lib.lib().spb_perm_dense_c128(ri.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        a.shape[0], ctypes.byref(opt), ctypes.byref(out))
+    _lib.check(st)
+    return _to_result(out, True)

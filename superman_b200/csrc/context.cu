@@ -1,0 +1,140 @@
+// Library-wide host state: error strings, per-device contexts, scratch arena.
+#include "context.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "spb_common.cuh"
+
+namespace {
+thread_local char g_last_error[512] = "";
+std::mutex g_ctx_mu;
+std::unique_ptr<spb::DeviceContext> g_ctx[64];
+}  // namespace
+
+void spb_set_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+extern "C" const char* spb_last_error(void) { return g_last_error; }
+
+extern "C" const char* spb_status_string(int status)
+{
+    switch (status) {
+    case SPB_OK: return "ok";
+    case SPB_ERR_INVALID: return "invalid argument";
+    case SPB_ERR_CUDA: return "cuda error";
+    case SPB_ERR_NO_DEVICE: return "no cuda device";
+    case SPB_ERR_OOM: return "out of memory";
+    case SPB_ERR_OVERFLOW: return "result overflow";
+    case SPB_ERR_TIMEOUT: return "timeout";
+    case SPB_ERR_CANCELLED: return "cancelled";
+    case SPB_ERR_BUSY: return "busy";
+    case SPB_ERR_IO: return "io error";
+    case SPB_ERR_NOT_SQUARE: return "matrix is not square";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int spb_version(void) { return 100; }
+
+extern "C" int spb_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" void spb_default_options(spb_options* opt)
+{
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->device = 0;
+    opt->precision = SPB_PREC_FP64;
+    opt->rel_tol = 0.0;
+}
+
+namespace spb {
+
+DeviceContext* get_context(int device, int* st)
+{
+    *st = SPB_OK;
+    if (device < 0 || device >= 64) {
+        spb_set_error("device ordinal %d out of range", device);
+        *st = SPB_ERR_INVALID;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (g_ctx[device]) return g_ctx[device].get();
+    int count = spb_device_count();
+    if (device >= count) {
+        spb_set_error("no CUDA device %d (%d visible)", device, count);
+        *st = SPB_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    auto ctx = std::make_unique<DeviceContext>();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_begin);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_end);
+    if (e != cudaSuccess) {
+        spb_set_error("device %d init failed: %s", device, cudaGetErrorString(e));
+        *st = SPB_ERR_CUDA;
+        return nullptr;
+    }
+    // Dynamic shared memory budget for the walk kernels: the opt-in limit less
+    // a reserve for their static shared arrays (reductions, flags).
+    ctx->smem_optin = optin > 4096 ? (size_t)optin - 4096 : (size_t)optin;
+    g_ctx[device] = std::move(ctx);
+    return g_ctx[device].get();
+}
+
+int ensure_scratch(DeviceContext* ctx, size_t bytes)
+{
+    if (bytes <= ctx->scratch_bytes) return SPB_OK;
+    if (ctx->scratch) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    size_t want = align_up(bytes < (1u << 20) ? (1u << 20) : bytes, 1u << 20);
+    if (cudaMalloc(&ctx->scratch, want) != cudaSuccess) {
+        cudaGetLastError();
+        spb_set_error("cudaMalloc of %zu scratch bytes failed", want);
+        return SPB_ERR_OOM;
+    }
+    ctx->scratch_bytes = want;
+    return SPB_OK;
+}
+
+int ensure_pinned(DeviceContext* ctx, size_t bytes)
+{
+    if (bytes <= ctx->pinned_bytes) return SPB_OK;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    size_t want = align_up(bytes < (1u << 16) ? (1u << 16) : bytes, 1u << 16);
+    if (cudaMallocHost(&ctx->pinned, want) != cudaSuccess) {
+        cudaGetLastError();
+        spb_set_error("cudaMallocHost of %zu bytes failed", want);
+        return SPB_ERR_OOM;
+    }
+    ctx->pinned_bytes = want;
+    return SPB_OK;
+}
+
+}  // namespace spb

@@ -1,0 +1,50 @@
+// Per-device runtime state shared by every entry point: a stream, timing
+// events, a grow-only device scratch arena and a pinned host staging buffer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <mutex>
+
+#include "superman_b200.h"
+
+namespace spb {
+
+struct DeviceContext {
+    int device = -1;
+    int sm_count = 0;
+    size_t smem_optin = 0;  // max dynamic shared memory per block (opt-in)
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    std::mutex mu;  // serialises calls that use this context
+};
+
+// Returns the context of `device`, creating it on first use (status in *st).
+DeviceContext* get_context(int device, int* st);
+
+// Ensures ctx->scratch holds at least `bytes` (grows, never shrinks).
+int ensure_scratch(DeviceContext* ctx, size_t bytes);
+
+// Ensures ctx->pinned holds at least `bytes` of page-locked host memory.
+int ensure_pinned(DeviceContext* ctx, size_t bytes);
+
+// Resolves the stream to use for a call.
+inline cudaStream_t call_stream(DeviceContext* ctx, const spb_options* opt)
+{
+    return (opt && opt->stream) ? static_cast<cudaStream_t>(opt->stream) : ctx->stream;
+}
+
+inline double wall_seconds()
+{
+    using clk = std::chrono::steady_clock;
+    return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
+}
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace spb

@@ -1,0 +1,302 @@
+// Dense real and complex permanents: Nijenhuis–Wilf Ryser with Gray-code
+// enumeration, restructured for sm_100a.
+//
+// Reference behaviour (paths relative to the SUPerman tree):
+//   x_i = a_{i,n-1} - rowsum_i / 2,   perm = (4(n%2)-2) * sum_S (-1)^|S| prod_i x_i(S)
+//   over the subsets S of columns 0..n-2, walked in Gray order
+//   (Algorithms/CPU/Dense/dpNaivePerman.h:53-141,
+//    Algorithms/GPU/Dense/DenseKernelDefinitions.cuh:189-264).
+//
+// B200 formulation.  The n-1 column bits of a subset index are split into
+//   low  w bits : enumerated from a shared-memory table DE[d][r] holding the
+//                 correctly rounded subset sums of the w lowest columns;
+//   high bits   : a "unit" index walked in Gray order per thread, with the
+//                 unit base vector xtop kept in double-double (hi in registers,
+//                 lo in shared memory).
+// Every term is x_r = fl(xtop_r + DE[d][r]) — one rounding from exact
+// values, so the row sums never drift (the reference accumulates x over
+// whole chunks, dpNaivePerman.h:125-129).  All lanes of a warp walk the same
+// d at the same time, so DE reads are shared-memory broadcasts.  Terms are
+// evaluated in groups of G consecutive d with compile-time signs; each unit's
+// FP64 sum is added to a per-thread double-double total, then reduced
+// warp -> block -> grid in a fixed order (deterministic).
+//
+// Rows are pre-scaled by exact powers of two (max |a_rj| in [0.5, 1)) and the
+// exponent sum is applied to the final result.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "context.h"
+#include "dense_impl.cuh"
+#include "spb_common.cuh"
+
+namespace spb {
+namespace dense {
+
+// ------------------------------------------------------------ setup kernel --
+// One CTA builds every table the walk kernels read.
+__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
+{
+    const int n = pb.n, c = pb.comps, w = pb.w, G = pb.g;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    __shared__ int s_exp[kMaxN];
+
+    // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in [0.5, 1).
+    for (int r = tid; r < n; r += bd) {
+        double mx = 0.0;
+        for (int j = 0; j < n * c; ++j) mx = fmax(mx, fabs(a_in[(size_t)r * n * c + j]));
+        int e = 0;
+        if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+        s_exp[r] = e;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < n * n * c; idx += bd) {
+        int r = idx / (n * c);
+        pb.as[idx] = ldexp(a_in[idx], -s_exp[r]);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int es = 0;
+        for (int r = 0; r < n; ++r) es += s_exp[r];
+        *pb.exp_sum = es;
+    }
+    // 2. NW start vector in double-double: x0_r = a'_{r,n-1} - rowsum'_r / 2.
+    for (int rr = tid; rr < n * c; rr += bd) {
+        int r = rr / c, part = rr % c;
+        dd s = {0.0, 0.0};
+        for (int j = 0; j < n; ++j) s = dd_add_d(s, pb.as[((size_t)r * n + j) * c + part]);
+        dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
+        dd x = dd_add_d(h, pb.as[((size_t)r * n + (n - 1)) * c + part]);
+        pb.x0_hi[part * n + r] = x.hi;
+        pb.x0_lo[part * n + r] = x.lo;
+    }
+    // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per part.
+    const int terms = 1 << w;
+    for (int idx = tid; idx < terms * n * c; idx += bd) {
+        int part = idx / (terms * n);
+        int rem = idx % (terms * n);
+        int d = rem / n, r = rem % n;
+        dd s = {0.0, 0.0};
+        for (int j = 0; j < w; ++j)
+            if ((d >> j) & 1) s = dd_add_d(s, pb.as[((size_t)r * n + j) * c + part]);
+        size_t pos = (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
+        pb.de_hi[pos] = s.hi;
+        pb.de_lo[pos] = s.lo;
+    }
+    // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
+    const int ntop = n - 1 - w;
+    for (int idx = tid; idx < ntop * n * c; idx += bd) {
+        int part = idx / (ntop * n);
+        int rem = idx % (ntop * n);
+        int j = rem / n, r = rem % n;
+        pb.mt[idx] = pb.as[((size_t)r * n + (w + j)) * c + part];
+        (void)part;
+    }
+}
+
+}  // namespace dense
+}  // namespace spb
+
+// ======================================================================
+// Host drivers
+// ======================================================================
+namespace spb {
+namespace dense {
+
+// Terms per group in the walk kernels; must equal RealCfg<N>::G /
+// ComplexCfg<N>::G, and the unit (2^w terms) must hold at least one group.
+int group_size(int n, int comps)
+{
+    if (comps == 1) return n >= 3 ? 4 : (n == 2 ? 2 : 1);
+    return n >= 2 ? 2 : 1;
+}
+
+int choose_unit_bits(int n, int comps, const spb_options* opt)
+{
+    int w;
+    if (opt && opt->unit_bits > 0) {
+        w = opt->unit_bits;
+    } else {
+        // Table budget 64 KB per part; keep >= 2^16 units when n allows.
+        w = 8;
+        while (w > 2 && ((size_t)1 << w) * n * 8 * comps > (size_t)64 * 1024) --w;
+        while (w > 2 && (n - 1 - w) < 16 && w > (n - 1) - 16) --w;
+    }
+    if (w > n - 1) w = n - 1;
+    const int g = group_size(n, comps);
+    const int wmin = g == 4 ? 2 : (g == 2 ? 1 : 0);
+    if (w < wmin) w = wmin;
+    return w;
+}
+
+// Sizes the scratch arena and fills the device pointers of *pb.
+size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
+{
+    const int n = pb->n, c = pb->comps;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    size_t o_in = take(sizeof(double) * n * n * c);
+    size_t o_as = take(sizeof(double) * n * n * c);
+    size_t o_x0h = take(sizeof(double) * n * c);
+    size_t o_x0l = take(sizeof(double) * n * c);
+    size_t terms = (size_t)1 << pb->w;
+    size_t o_deh = take(sizeof(double) * terms * n * c);
+    size_t o_del = take(sizeof(double) * terms * n * c);
+    size_t o_mt = take(sizeof(double) * (size_t)(n - 1 - pb->w > 0 ? n - 1 - pb->w : 1) * n * c);
+    size_t o_part = take(sizeof(dd) * (size_t)pb->grid * c);
+    size_t o_tick = take(sizeof(unsigned) * 4);
+    size_t o_res = take(sizeof(dd) * 2);
+    size_t o_exp = take(sizeof(int) * 4);
+    if (base) {
+        pb->as = reinterpret_cast<double*>(base + o_as);
+        pb->x0_hi = reinterpret_cast<double*>(base + o_x0h);
+        pb->x0_lo = reinterpret_cast<double*>(base + o_x0l);
+        pb->de_hi = reinterpret_cast<double*>(base + o_deh);
+        pb->de_lo = reinterpret_cast<double*>(base + o_del);
+        pb->mt = reinterpret_cast<double*>(base + o_mt);
+        pb->partials = reinterpret_cast<dd*>(base + o_part);
+        pb->ticket = reinterpret_cast<unsigned*>(base + o_tick);
+        pb->result = reinterpret_cast<dd*>(base + o_res);
+        pb->exp_sum = reinterpret_cast<int*>(base + o_exp);
+    }
+    if (in_offset) *in_offset = o_in;
+    return off;
+}
+
+size_t walk_smem_bytes(const Problem& pb, int threads)
+{
+    const int n = pb.n, c = pb.comps;
+    size_t terms = (size_t)1 << pb.w;
+    int ntop = n - 1 - pb.w;
+    return sizeof(double) * (terms * n * c + (size_t)(ntop > 0 ? ntop : 0) * n * c +
+                             (size_t)n * c * threads);
+}
+
+static int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in,
+               spb_result* out)
+{
+    double t_start = wall_seconds();
+    if (!out) {
+        spb_set_error("null result pointer");
+        return SPB_ERR_INVALID;
+    }
+    std::memset(out, 0, sizeof(*out));
+    spb_options opt;
+    if (opt_in) opt = *opt_in; else spb_default_options(&opt);
+    if (!a || n < 1 || n > kMaxN) {
+        spb_set_error("dense permanent needs a non-null matrix and 1 <= n <= %d (got n=%d)", kMaxN, n);
+        return out->status = SPB_ERR_INVALID;
+    }
+    int st = SPB_OK;
+    DeviceContext* ctx = get_context(opt.device, &st);
+    if (!ctx) return out->status = st;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SPB_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t stream = call_stream(ctx, &opt);
+
+    Problem pb{};
+    pb.n = n;
+    pb.comps = comps;
+    pb.w = choose_unit_bits(n, comps, &opt);
+    pb.g = group_size(n, comps);
+    pb.units = 1ull << (n - 1 - pb.w);
+
+    int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 0;
+    const int max_threads = walk_max_threads(n, comps);
+    if (threads == 0) {
+        threads = max_threads;
+        // fit the per-thread lo vectors next to the tables
+        while (threads > 64 && walk_smem_bytes(pb, threads) > ctx->smem_optin) threads -= 32;
+    }
+    if (threads > max_threads) threads = max_threads;
+    threads = (threads / 32) * 32;
+    if (threads < 32) threads = 32;
+    size_t smem = walk_smem_bytes(pb, threads);
+    if (smem > ctx->smem_optin) {
+        spb_set_error("dense n=%d: %zu B shared memory exceeds the %zu B limit", n, smem, ctx->smem_optin);
+        return out->status = SPB_ERR_INVALID;
+    }
+    int blocks = opt.blocks > 0 ? opt.blocks : ctx->sm_count;
+    // never launch more threads than units
+    unsigned long long max_blocks = (pb.units + threads - 1) / threads;
+    if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
+    if (blocks < 1) blocks = 1;
+    pb.grid = blocks;
+
+    size_t in_off = 0;
+    size_t need = plan_layout(&pb, nullptr, &in_off);
+    if ((st = ensure_scratch(ctx, need)) != SPB_OK) return out->status = st;
+    char* base = static_cast<char*>(ctx->scratch);
+    plan_layout(&pb, base, &in_off);
+    const double* d_a = a;
+    if (!a_on_device) {
+        double* d_in = reinterpret_cast<double*>(base + in_off);
+        SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, sizeof(double) * n * n * comps,
+                                     cudaMemcpyHostToDevice, stream));
+        d_a = d_in;
+    }
+    SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
+    setup_kernel<<<1, 512, 0, stream>>>(pb, d_a);
+    SPB_CUDA_TRY(cudaGetLastError());
+    SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
+    st = launch_walk(pb, blocks, threads, smem, stream);
+    if (st != SPB_OK) return out->status = st;
+    SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
+
+    struct {
+        dd res[2];
+        int e;
+    } h;
+    SPB_CUDA_TRY(cudaMemcpyAsync(h.res, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
+    SPB_CUDA_TRY(cudaMemcpyAsync(&h.e, pb.exp_sum, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
+
+    // perm = (4(n%2)-2) * total * 2^E ; the factor is +-2, an exact power of two.
+    const int e = h.e + 1;
+    const double sgn = (n % 2) ? 1.0 : -1.0;
+    out->value = sgn * std::ldexp(h.res[0].hi, e);
+    out->value_lo = sgn * std::ldexp(h.res[0].lo, e);
+    if (comps == 2) {
+        out->imag = sgn * std::ldexp(h.res[1].hi, e);
+        out->imag_lo = sgn * std::ldexp(h.res[1].lo, e);
+    }
+    out->kernel_s = ms * 1e-3;
+    out->gray_steps = (uint64_t)n << (n - 1);
+    out->launches = 2;
+    out->status = SPB_OK;
+    out->elapsed_s = wall_seconds() - t_start;
+    return SPB_OK;
+}
+
+}  // namespace dense
+}  // namespace spb
+
+extern "C" int spb_perm_dense_f64(const double* a, int n, const spb_options* opt, spb_result* out)
+{
+    return spb::dense::run(a, false, n, 1, opt, out);
+}
+
+extern "C" int spb_perm_dense_f64_dev(const double* d_a, int n, const spb_options* opt,
+                                      spb_result* out)
+{
+    return spb::dense::run(d_a, true, n, 1, opt, out);
+}
+
+extern "C" int spb_perm_dense_c128(const double* a, int n, const spb_options* opt, spb_result* out)
+{
+    return spb::dense::run(a, false, n, 2, opt, out);
+}
+
+extern "C" int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options* opt,
+                                       spb_result* out)
+{
+    return spb::dense::run(d_a, true, n, 2, opt, out);
+}

@@ -1,0 +1,340 @@
+// Dense walk kernels (real and complex), shared between the driver in
+// dense.cu and the per-n instantiation units dense_walk_{real,complex}.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "spb_common.cuh"
+
+namespace spb {
+namespace dense {
+
+constexpr int kMaxN = 63;
+
+// Device-side description of one permanent: sizes plus pointers into the
+// scratch arena written by setup_kernel.
+struct Problem {
+    int n, comps, w, g, grid;
+    unsigned long long units;  // 2^(n-1-w) Gray units of 2^w terms each
+    double* as;                // row-scaled matrix (row-major, comps interleaved)
+    double* x0_hi;             // [comps][n] NW start vector, double-double
+    double* x0_lo;
+    double* de_hi;             // [comps][2^w/G][n][G] low-column subset sums
+    double* de_lo;             // rounding residues of de_hi
+    double* mt;                // [comps][n-1-w][n] high columns
+    dd* partials;              // [comps][grid] per-CTA sums
+    unsigned* ticket;          // last-CTA election counter (reset by the kernel)
+    dd* result;                // [comps] grid total
+    int* exp_sum;              // sum of the row scaling exponents
+};
+
+// Thread caps keep the x vector (2 registers per double) plus the product
+// chains under the per-thread register budget the cap implies
+// (65536 / threads), so the walk never spills at the sizes that matter.
+__host__ __device__ constexpr int RealMaxThreads(int n) { return n <= 40 ? 512 : 256; }
+__host__ __device__ constexpr int ComplexMaxThreads(int n) { return n <= 14 ? 512 : (n <= 26 ? 384 : 256); }
+
+template <int N>
+struct RealCfg {
+    static constexpr int G = N >= 3 ? 4 : (N == 2 ? 2 : 1);
+    static constexpr int kMaxThreads = RealMaxThreads(N);
+};
+
+template <int N>
+struct ComplexCfg {
+    static constexpr int G = N >= 2 ? 2 : 1;
+    static constexpr int kMaxThreads = ComplexMaxThreads(N);
+};
+
+__device__ __forceinline__ dd ldcg_dd(const dd* p)
+{
+    return {__ldcg(&p->hi), __ldcg(&p->lo)};
+}
+
+// Warp -> block -> grid double-double reduction of C components.  The last
+// CTA to finish (ticket election) sums the per-CTA partials in index order,
+// so the result does not depend on CTA completion order.
+template <int C>
+__device__ __forceinline__ void grid_reduce(dd (&tot)[C], const Problem& pb)
+{
+    __shared__ dd s_warp[C][32];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int c = 0; c < C; ++c) tot[c] = warp_sum_dd(tot[c]);
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) s_warp[c][wid] = tot[c];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            dd v = lane < nw ? s_warp[c][lane] : dd{0.0, 0.0};
+            v = warp_sum_dd(v);
+            if (lane == 0) pb.partials[c * pb.grid + blockIdx.x] = v;
+        }
+        if (lane == 0) {
+            __threadfence();
+            unsigned prev = atomicAdd(pb.ticket, 1u);
+            s_last = (prev == gridDim.x - 1) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    if (s_last && wid == 0) {
+        __threadfence();
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            dd v = {0.0, 0.0};
+            for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + c * pb.grid + b));
+            v = warp_sum_dd(v);
+            if (lane == 0) pb.result[c] = v;
+        }
+        if (lane == 0) *pb.ticket = 0u;
+    }
+}
+
+// ---------------------------------------------------------------- real ----
+// Sum over one unit: sum_d (-1)^popc(d) prod_r (xh_r + DE[d][r]).
+template <int N, int G>
+__device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const double* __restrict__ s_de,
+                                                int nq)
+{
+    double acc = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < nq; ++q) {
+        const double* de = s_de + q * (N * G);
+        double p[G];
+        if constexpr (G == 4) {
+            double2 v0 = reinterpret_cast<const double2*>(de)[0];
+            double2 v1 = reinterpret_cast<const double2*>(de)[1];
+            p[0] = add_rn(xh[0], v0.x);
+            p[1] = add_rn(xh[0], v0.y);
+            p[2] = add_rn(xh[0], v1.x);
+            p[3] = add_rn(xh[0], v1.y);
+#pragma unroll
+            for (int r = 1; r < N; ++r) {
+                double2 a = reinterpret_cast<const double2*>(de + r * 4)[0];
+                double2 b = reinterpret_cast<const double2*>(de + r * 4)[1];
+                p[0] = mul_rn(p[0], add_rn(xh[r], a.x));
+                p[1] = mul_rn(p[1], add_rn(xh[r], a.y));
+                p[2] = mul_rn(p[2], add_rn(xh[r], b.x));
+                p[3] = mul_rn(p[3], add_rn(xh[r], b.y));
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < G; ++i) p[i] = add_rn(xh[0], de[i]);
+#pragma unroll
+            for (int r = 1; r < N; ++r) {
+#pragma unroll
+                for (int i = 0; i < G; ++i) p[i] = mul_rn(p[i], add_rn(xh[r], de[r * G + i]));
+            }
+        }
+        double gs;
+        if constexpr (G == 4) gs = sub_rn(sub_rn(p[0], p[1]), sub_rn(p[2], p[3]));  // + - - +
+        else if constexpr (G == 2) gs = sub_rn(p[0], p[1]);
+        else gs = p[0];
+        acc = (__popc(q) & 1) ? sub_rn(acc, gs) : add_rn(acc, gs);
+    }
+    return acc;
+}
+
+template <int N>
+__global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem pb)
+{
+    constexpr int G = RealCfg<N>::G;
+    extern __shared__ __align__(16) double smem[];
+    const int w = pb.w;
+    const int terms = 1 << w;
+    const int nq = terms / G;
+    const int ntop = N - 1 - w;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    double* s_de = smem;
+    double* s_mt = s_de + terms * N;
+    double* s_lo = s_mt + (ntop > 0 ? ntop : 0) * N;
+    for (int i = tid; i < terms * N; i += bd) s_de[i] = pb.de_hi[i];
+    for (int i = tid; i < ntop * N; i += bd) s_mt[i] = pb.mt[i];
+    __syncthreads();
+
+    const unsigned long long T = (unsigned long long)gridDim.x * bd;
+    const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
+    unsigned long long u0, u1;
+    balanced_range(pb.units, T, t, &u0, &u1);
+    dd tot[1] = {{0.0, 0.0}};
+    if (u0 < u1) {
+        double xh[N];
+        const unsigned long long g0 = gray_of(u0);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            dd x = {pb.x0_hi[r], pb.x0_lo[r]};
+            for (int j = 0; j < ntop; ++j)
+                if ((g0 >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
+            xh[r] = x.hi;
+            s_lo[r * bd + tid] = x.lo;
+        }
+        unsigned long long u = u0;
+        while (true) {
+            double us = unit_sum_real<N, G>(xh, s_de, nq);
+            tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
+            if (++u >= u1) break;
+            const int j = __ffsll((long long)u) - 1;
+            const bool add = (gray_of(u) >> j) & 1ull;
+            const double* col = s_mt + j * N;
+#pragma unroll
+            for (int r = 0; r < N; ++r) {
+                double m = add ? col[r] : -col[r];
+                dd s = two_sum(xh[r], m);
+                dd z = fast_two_sum(s.hi, add_rn(s.lo, s_lo[r * bd + tid]));
+                xh[r] = z.hi;
+                s_lo[r * bd + tid] = z.lo;
+            }
+        }
+    }
+    grid_reduce<1>(tot, pb);
+}
+
+// ------------------------------------------------------------- complex ----
+template <int N, int G>
+__device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const double (&xi)[N],
+                                                 const double* __restrict__ s_de_re,
+                                                 const double* __restrict__ s_de_im, int nq,
+                                                 double& acc_re, double& acc_im)
+{
+    double ar = 0.0, ai = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < nq; ++q) {
+        const double* dr = s_de_re + q * (N * G);
+        const double* di = s_de_im + q * (N * G);
+        double pr[G], pi[G];
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            pr[i] = add_rn(xr[0], dr[i]);
+            pi[i] = add_rn(xi[0], di[i]);
+        }
+#pragma unroll
+        for (int r = 1; r < N; ++r) {
+            double vr[G], vi[G];
+            if constexpr (G == 2) {
+                double2 a = reinterpret_cast<const double2*>(dr + r * 2)[0];
+                double2 b = reinterpret_cast<const double2*>(di + r * 2)[0];
+                vr[0] = a.x; vr[1] = a.y; vi[0] = b.x; vi[1] = b.y;
+            } else {
+#pragma unroll
+                for (int i = 0; i < G; ++i) { vr[i] = dr[r * G + i]; vi[i] = di[r * G + i]; }
+            }
+#pragma unroll
+            for (int i = 0; i < G; ++i) {
+                double yr = add_rn(xr[r], vr[i]);
+                double yi = add_rn(xi[r], vi[i]);
+                double t1 = mul_rn(pi[i], yi);
+                double t2 = mul_rn(pi[i], yr);
+                double nr = __fma_rn(pr[i], yr, -t1);
+                double ni = __fma_rn(pr[i], yi, t2);
+                pr[i] = nr;
+                pi[i] = ni;
+            }
+        }
+        double gr, gi;
+        if constexpr (G == 2) { gr = sub_rn(pr[0], pr[1]); gi = sub_rn(pi[0], pi[1]); }
+        else { gr = pr[0]; gi = pi[0]; }
+        if (__popc(q) & 1) { ar = sub_rn(ar, gr); ai = sub_rn(ai, gi); }
+        else { ar = add_rn(ar, gr); ai = add_rn(ai, gi); }
+    }
+    acc_re = ar;
+    acc_im = ai;
+}
+
+template <int N>
+__global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Problem pb)
+{
+    constexpr int G = ComplexCfg<N>::G;
+    extern __shared__ __align__(16) double smem[];
+    const int w = pb.w;
+    const int terms = 1 << w;
+    const int nq = terms / G;
+    const int ntop = N - 1 - w;
+    const int ntp = ntop > 0 ? ntop : 0;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    double* s_de = smem;                        // [2][terms*N]
+    double* s_mt = s_de + 2 * terms * N;        // [2][ntop*N]
+    double* s_lo = s_mt + 2 * ntp * N;          // [2][N][bd]
+    for (int i = tid; i < 2 * terms * N; i += bd) s_de[i] = pb.de_hi[i];
+    for (int i = tid; i < 2 * ntp * N; i += bd) s_mt[i] = pb.mt[i];
+    __syncthreads();
+    const double* s_mt_re = s_mt;
+    const double* s_mt_im = s_mt + ntp * N;
+    double* s_lo_re = s_lo;
+    double* s_lo_im = s_lo + N * bd;
+
+    const unsigned long long T = (unsigned long long)gridDim.x * bd;
+    const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
+    unsigned long long u0, u1;
+    balanced_range(pb.units, T, t, &u0, &u1);
+    dd tot[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    if (u0 < u1) {
+        double xr[N], xi[N];
+        const unsigned long long g0 = gray_of(u0);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            dd a = {pb.x0_hi[r], pb.x0_lo[r]};
+            dd b = {pb.x0_hi[N + r], pb.x0_lo[N + r]};
+            for (int j = 0; j < ntop; ++j)
+                if ((g0 >> j) & 1ull) {
+                    a = dd_add_d(a, s_mt_re[j * N + r]);
+                    b = dd_add_d(b, s_mt_im[j * N + r]);
+                }
+            xr[r] = a.hi;
+            xi[r] = b.hi;
+            s_lo_re[r * bd + tid] = a.lo;
+            s_lo_im[r * bd + tid] = b.lo;
+        }
+        unsigned long long u = u0;
+        while (true) {
+            double ur, ui;
+            unit_sum_complex<N, G>(xr, xi, s_de, s_de + terms * N, nq, ur, ui);
+            if (u & 1ull) { ur = -ur; ui = -ui; }
+            tot[0] = dd_add_d(tot[0], ur);
+            tot[1] = dd_add_d(tot[1], ui);
+            if (++u >= u1) break;
+            const int j = __ffsll((long long)u) - 1;
+            const bool add = (gray_of(u) >> j) & 1ull;
+#pragma unroll
+            for (int r = 0; r < N; ++r) {
+                double mr = add ? s_mt_re[j * N + r] : -s_mt_re[j * N + r];
+                double mi = add ? s_mt_im[j * N + r] : -s_mt_im[j * N + r];
+                dd s = two_sum(xr[r], mr);
+                dd z = fast_two_sum(s.hi, add_rn(s.lo, s_lo_re[r * bd + tid]));
+                xr[r] = z.hi;
+                s_lo_re[r * bd + tid] = z.lo;
+                s = two_sum(xi[r], mi);
+                z = fast_two_sum(s.hi, add_rn(s.lo, s_lo_im[r * bd + tid]));
+                xi[r] = z.hi;
+                s_lo_im[r * bd + tid] = z.lo;
+            }
+        }
+    }
+    grid_reduce<2>(tot, pb);
+}
+
+// Per-n dispatch (defined in the instantiation units).
+int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+int launch_walk_complex(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+
+inline int launch_walk(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s)
+{
+    return pb.comps == 1 ? launch_walk_real(pb, blocks, threads, smem, s)
+                         : launch_walk_complex(pb, blocks, threads, smem, s);
+}
+
+int walk_max_threads(int n, int comps);
+
+}  // namespace dense
+}  // namespace spb
+
+// X-macro over n = 1..63.
+#define SPB_FOR_EACH_N(X)                                                                  \
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15)       \
+    X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29)    \
+    X(30) X(31) X(32) X(33) X(34) X(35) X(36) X(37) X(38) X(39) X(40) X(41) X(42) X(43)    \
+    X(44) X(45) X(46) X(47) X(48) X(49) X(50) X(51) X(52) X(53) X(54) X(55) X(56) X(57)    \
+    X(58) X(59) X(60) X(61) X(62) X(63)
