@@ -1,0 +1,361 @@
+"""Benchmark of the Ryser / Gray-code permanent hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dense32|dense24|complex28|binary36|sparse40]
+
+A step is one permanent of the workload matrix (the headline: dense real FP64
+n=32, entries U[0,1) from SplitMix64 seed 7).  The metric is Gray steps per
+second, n*2^(n-1) per permanent (the reference's own unit of work, the NW
+Gray walk of Algorithms/CPU/Dense/dpNaivePerman.h:116-133), summed over all
+ranks.  Multi-GPU runs are independent replicas (the path has no data
+exchange; one process per GPU, max-over-ranks device time).
+
+Printed JSON line (rank 0):
+  value      device-resident input, CUDA-event time per step on the launch stream
+  e2e        same metric through the C ABI with a pinned host matrix: H2D copy,
+             kernels, D2H of the result inside the timed region
+  roofline   dominant kernel (the Gray walk): FP64 pipe instructions per
+             launch / walk-kernel time, against the FP64 FMA pipe peak measured
+             by a DFMA microbenchmark in the same run
+  cpu_baseline  the reference's CPU Ryser (oracle/_ref) on this host's cores
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (kind, n, seed, description)
+    "dense32": ("dense", 32, 7, "dense_f64_u01_n32_seed7"),
+    "dense24": ("dense", 24, 3, "dense_f64_u01_n24_seed3"),
+    "dense28": ("dense", 28, 28, "dense_f64_u01_n28_seed28"),
+    "complex28": ("complex", 28, 6, "complex128_haar256_block_n28_seed6"),
+}
+
+# DRAM bytes per walk launch from one ncu capture of this workload
+# (profiles/dense_walk_n32.md); None until captured.
+NCU_TRAFFIC = {"dense32": None}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+        0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+        0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+        0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device: int, period_s: float = 0.005):
+        self.device, self.period = device, period_s
+        self.samples, self.reasons = [], 0
+        self._stop = threading.Event()
+        self._thread = None
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # no NVML: report no clocks rather than fail
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                self.reasons |= nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if self._nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        names = [v for k, v in self.REASONS.items() if self.reasons & k and v != "gpu_idle"]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": names, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------- reference (CPU) arm --
+def write_mtx(path, a):
+    import numpy as np
+    n = a.shape[0]
+    lines = []
+    cplx = np.iscomplexobj(a)
+    for i in range(n):
+        for j in range(n):
+            v = a[i, j]
+            if v == 0:
+                continue
+            if cplx:
+                lines.append(f"{i + 1} {j + 1} {float(v.real)!r} {float(v.imag)!r}")
+            else:
+                lines.append(f"{i + 1} {j + 1} {float(v)!r}")
+    with open(path, "w") as f:
+        f.write(f"{n} {n} {len(lines)}\n" + "\n".join(lines) + "\n")
+
+
+def reference_step(a, threads, complex_=False, timeout=1800):
+    """One run of the reference CPU binary; returns its own reported seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "m.mtx")
+        write_mtx(p, a)
+        extra = ["complex=true"] if complex_ else []
+        _, secs = O.run_reference(p, threads=threads, extra=extra, timeout=timeout)
+    return secs
+
+
+def port_step(a, threads, complex_=False):
+    """Fallback when the reference binary is absent: the oracle's restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    if complex_:
+        O.complex_nw(a, threads=threads)
+    else:
+        O.dense_nw(a, threads=threads)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(kind, n, seed, cores):
+    """Bounded CPU sample of the workload: the same generator at the largest
+    n' <= n whose estimated reference time is <= ~20 s on `cores` threads
+    (dense: ~1e10 Gray steps/s on 8 cores, scaling with cores)."""
+    rate = 1.2e9 * cores * (0.3 if kind == "complex" else 1.0)
+    m = n
+    while m > 12 and m * 2 ** (m - 1) / rate > 20.0:
+        m -= 1
+    return m
+
+
+def make_matrix(kind, n, seed):
+    from superman_b200 import workloads as W
+    if kind == "dense":
+        return W.dense_uniform(n, seed)
+    if kind == "complex":
+        return W.haar_block(n, seed)
+    raise ValueError(kind)
+
+
+def run_cpu_baseline(kind, n, seed, steps=1):
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "superman_ref")
+    cores = os.cpu_count() or 1
+    m = cpu_sample(kind, n, seed, cores)
+    a = make_matrix(kind, m, seed)
+    use_ref = os.path.exists(ref_bin)
+    times = []
+    for _ in range(steps):
+        times.append(reference_step(a, cores, kind == "complex") if use_ref
+                     else port_step(a, cores, kind == "complex"))
+    t = statistics.mean(times)
+    return {"value": m * 2 ** (m - 1) / t, "unit": "gray-steps/s", "cores": cores,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"one full permanent of the same generator at n={m} "
+                      f"({'reference CPU binary oracle/_ref, mode=cpu' if use_ref else 'oracle port'}, "
+                      f"thread_count={cores}); mean of {steps} run(s), {t:.3f} s each"}, times
+
+
+def reference_arm(args, wl):
+    kind, n, seed, desc = WORKLOADS[wl]
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    for _ in range(args.warmup):
+        run_cpu_baseline(kind, n, seed, steps=1)
+    cb, times = run_cpu_baseline(kind, n, seed, steps=args.steps)
+    t = statistics.mean(times)
+    line = {"metric": "ryser_gray_steps_per_s", "value": cb["value"], "unit": "gray-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "kind": kind, "n": n, "seed": seed},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "gray-steps/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- our GPU arm --
+def ours_arm(args, wl):
+    import numpy as np
+    import torch
+    import superman_b200 as S
+    from superman_b200 import _lib
+
+    kind, n, seed, desc = WORKLOADS[wl]
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    device = local
+    torch.cuda.set_device(device)
+    L = _lib.lib()
+
+    a = make_matrix(kind, n, seed)
+    comps = 2 if kind == "complex" else 1
+    host = torch.from_numpy(np.ascontiguousarray(a).view(np.float64).copy()).pin_memory()
+    dev_a = host.to(f"cuda:{device}")
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{device}")
+    # The library runs on its own stream and times each call with CUDA events
+    # recorded on that stream (spb_result.device_s / kernel_s).
+    opt = _lib.default_options(device=device, precision=_lib.SPB_PREC_DD if args.precision == "dd"
+                               else _lib.SPB_PREC_FP64)
+    res = _lib.spb_result()
+    fn_dev = L.spb_perm_dense_c128_dev if comps == 2 else L.spb_perm_dense_f64_dev
+    fn_host = L.spb_perm_dense_c128 if comps == 2 else L.spb_perm_dense_f64
+    host_ptr = ctypes.cast(ctypes.c_void_p(host.data_ptr()), ctypes.POINTER(ctypes.c_double))
+
+    peak = ctypes.c_double()
+    _lib.check(L.spb_measure_pipe_peak(device, 0, ctypes.byref(peak)))
+
+    def step_dev():
+        _lib.check(fn_dev(ctypes.c_void_p(dev_a.data_ptr()), n, ctypes.byref(opt), ctypes.byref(res)))
+        return res.device_s, res.kernel_s, res.launches
+
+    def step_host():
+        _lib.check(fn_host(host_ptr, n, ctypes.byref(opt), ctypes.byref(res)))
+        return res.device_s, res.kernel_s, res.launches
+
+    def timed(step):
+        for _ in range(args.warmup):
+            flush.zero_()
+            torch.cuda.synchronize()
+            step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        total_ms, walk_s, launches = 0.0, 0.0, 0
+        for _ in range(args.steps):
+            flush.zero_()  # evict L2 between steps (outside the step's events)
+            torch.cuda.synchronize()
+            ds, ks, nl = step()  # returns after its own stream synchronize
+            total_ms += ds * 1e3
+            walk_s += ks
+            launches += nl
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+            t = torch.tensor([total_ms, walk_s], device=f"cuda:{device}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms, walk_s = t[0].item(), t[1].item()
+        return total_ms / args.steps, walk_s / args.steps, launches
+
+    with ClockSampler(device) as clk:
+        ms_dev, walk_dev, launches = timed(step_dev)
+    value_dev = float(res.value) + 1j * float(res.imag) if comps == 2 else float(res.value)
+    ms_e2e, _, _ = timed(step_host)
+
+    steps_per_perm = n * 2 ** (n - 1)
+    value = world * steps_per_perm / (ms_dev * 1e-3)
+    e2e = world * steps_per_perm / (ms_e2e * 1e-3)
+    fp64_per_row = 2 if comps == 1 else 6  # DADD+DMUL (real); 2 DADD+2 DMUL+2 DFMA (complex)
+    alg = fp64_per_row * steps_per_perm  # FP64 pipe instructions per walk launch
+    achieved = alg / walk_dev
+    roofline = {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
+                "unit": "T FP64-pipe inst/s", "frac": achieved / peak.value,
+                "traffic": NCU_TRAFFIC.get(wl),
+                "peak_source": "DFMA microbenchmark in this run (spb_measure_pipe_peak); "
+                               "MEASURED_PEAKS.json has no FP64 figure",
+                "algorithmic_per_launch": alg}
+
+    err = None
+    golden_name = {"dense32": "dense_u01_n32_s7", "dense24": "dense_u01_n24_s3",
+                   "complex28": "complex_haar_n28_s6"}.get(wl)
+    golden = os.path.join(ROOT, "tests", "golden", f"{golden_name}.json")
+    if golden_name and os.path.exists(golden) and rank == 0:
+        from fractions import Fraction
+        g = json.load(open(golden))
+        if comps == 1 and [float(v).hex() for v in a.ravel()] == g["hex"]:
+            ex = Fraction(g["exact"])
+            err = float(abs(Fraction(value_dev) - ex) / abs(ex))
+        elif comps == 2 and [float(v.real).hex() for v in a.ravel()] == g["re_hex"]:
+            er, ei = Fraction(g["exact_re"]), Fraction(g["exact_im"])
+            d2 = (Fraction(value_dev.real) - er) ** 2 + (Fraction(value_dev.imag) - ei) ** 2
+            err = math.sqrt(float(d2 / (er * er + ei * ei)))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _ = run_cpu_baseline(kind, n, seed, steps=1)
+
+    line = {"metric": "ryser_gray_steps_per_s", "value": value, "unit": "gray-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_dev, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "kind": kind, "n": n, "seed": seed,
+                       "precision": args.precision, "l2": "flushed between steps (256 MiB write)",
+                       "permanent": repr(value_dev), "rel_err_vs_exact": err},
+            "e2e": {"value": e2e, "unit": "gray-steps/s", "h2d_bytes_per_step": n * n * 8 * comps,
+                    "d2h_bytes_per_step": 16 * comps + 4},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": launches}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dense32")
+    ap.add_argument("--precision", choices=["fp64", "dd"], default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args, args.workload)
+    return ours_arm(args, args.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -276,16 +276,19 @@ def ref_binary_path() -> str:
     return _REF_BIN
 
 
-def run_reference(mtx_path: str, threads=None, extra=()):
+def run_reference(mtx_path: str, threads=None, extra=(), timeout=3600):
     """Run the reference's own CPU program on a matrix file; returns
-    (permanent as float or complex, seconds).  Needs oracle/_ref built."""
+    (permanent as float or complex, seconds).  Needs oracle/_ref built.
+    Each run gets a fresh mailbox directory: the reference blocks while an
+    unread mailbox file exists (CommonFiles/Helpers.h:71-116)."""
     import re
     import tempfile
     work = tempfile.mkdtemp(prefix="spb_ref_")
     os.makedirs(os.path.join(work, "build"), exist_ok=True)
     args = [_REF_BIN, "pid=2", f"repo_dir={work}/", f"filename={mtx_path}", "mode=cpu",
             f"thread_count={_threads(threads)}", *extra]
-    out = subprocess.run(args, check=True, capture_output=True, text=True).stdout
+    out = subprocess.run(args, check=True, capture_output=True, text=True,
+                         timeout=timeout).stdout
     m2 = re.search(r"Permanent: \(([^,]+),([^)]+)\) - Computed in: (\S+) seconds", out)
     if m2 is not None:
         return complex(float(m2.group(1)), float(m2.group(2))), float(m2.group(3))
