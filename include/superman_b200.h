@@ -67,6 +67,8 @@ typedef struct spb_result {
     double imag_lo;
     double elapsed_s;      /* wall time of the whole call                   */
     double kernel_s;       /* device time of the Gray-walk kernels          */
+    double device_s;       /* device time of the whole call on its stream:
+                              input copy (if any), kernels, result copy     */
     double err_est;        /* estimated relative error (statistical)        */
     uint64_t gray_steps;   /* Gray steps walked: n*2^(n-1) (NW) or n*2^n    */
     uint64_t refined_units;/* units re-evaluated in double-double           */

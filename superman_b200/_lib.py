@@ -59,6 +59,7 @@ class spb_result(ctypes.Structure):
         ("imag_lo", ctypes.c_double),
         ("elapsed_s", ctypes.c_double),
         ("kernel_s", ctypes.c_double),
+        ("device_s", ctypes.c_double),
         ("err_est", ctypes.c_double),
         ("gray_steps", ctypes.c_uint64),
         ("refined_units", ctypes.c_uint64),

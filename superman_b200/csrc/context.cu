@@ -90,6 +90,8 @@ DeviceContext* get_context(int device, int* st)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_begin);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_end);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_call0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_call1);
     if (e != cudaSuccess) {
         spb_set_error("device %d init failed: %s", device, cudaGetErrorString(e));
         *st = SPB_ERR_CUDA;

@@ -16,7 +16,8 @@ struct DeviceContext {
     int sm_count = 0;
     size_t smem_optin = 0;  // max dynamic shared memory per block (opt-in)
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;      // around the walk kernels
+    cudaEvent_t ev_call0 = nullptr, ev_call1 = nullptr;    // around the whole call
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     void* pinned = nullptr;
