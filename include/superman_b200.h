@@ -114,6 +114,21 @@ SPB_API int spb_perm_dense_c128(const double* a, int n, const spb_options* opt, 
 SPB_API int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options* opt,
                             spb_result* out);
 
+/* Dense real permanent that allocates nothing, for callers that cannot let a
+ * library call cudaMalloc/cudaFree: programs that reserve all device memory
+ * for their own pool allocator, and latency-bound request loops that cannot
+ * take cudaFree's device-wide synchronisation or an allocation failure
+ * mid-request.  d_a: device, n*n doubles row-major; d_out: device, 2 doubles
+ * receiving the permanent as a double-double (hi, lo).  Runs asynchronously
+ * on `stream` (NULL = the default stream); read d_out after synchronising.
+ * Working memory is one fixed 256 KiB device array per GPU inside the
+ * library, so n is limited to 1..40 (larger n: SPB_ERR_INVALID).  The first
+ * call on a device looks up that array's address (make it before any stream
+ * capture).  All calls share the array: calls that overlap on the GPU race.
+ * No counterpart in the reference, which allocates on every call
+ * (Algorithms/GPU/Dense/dpSingleGPU.cuh:138-144). */
+SPB_API int spb_perm_dense_f64_noalloc(const double* d_a, int n, double* d_out, void* stream);
+
 /* Measured pipe throughput used as the roofline denominator: which = 0 gives
  * FP64 FMA thread-instructions per second, which = 1 gives int32 multiply-add
  * thread-instructions per second (best of three timed launches).  No

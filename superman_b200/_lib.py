@@ -83,6 +83,8 @@ SIGNATURES = {
     "spb_perm_dense_f64_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128": (ctypes.c_int, [_DP, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),
+    "spb_perm_dense_f64_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_void_p]),
     "spb_measure_pipe_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_double)]),
 }
