@@ -92,6 +92,8 @@ DeviceContext* get_context(int device, int* st)
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_end);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_call0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_call1);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_ref0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_ref1);
     if (e != cudaSuccess) {
         spb_set_error("device %d init failed: %s", device, cudaGetErrorString(e));
         *st = SPB_ERR_CUDA;
@@ -120,6 +122,25 @@ int ensure_scratch(DeviceContext* ctx, size_t bytes)
         return SPB_ERR_OOM;
     }
     ctx->scratch_bytes = want;
+    return SPB_OK;
+}
+
+int ensure_list(DeviceContext* ctx, size_t bytes)
+{
+    if (bytes <= ctx->list_bytes) return SPB_OK;
+    if (ctx->list) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->list);
+        ctx->list = nullptr;
+        ctx->list_bytes = 0;
+    }
+    size_t want = align_up(bytes, 1u << 20);
+    if (cudaMalloc(&ctx->list, want) != cudaSuccess) {
+        cudaGetLastError();
+        spb_set_error("cudaMalloc of %zu refinement-list bytes failed", want);
+        return SPB_ERR_OOM;
+    }
+    ctx->list_bytes = want;
     return SPB_OK;
 }
 

@@ -18,6 +18,9 @@ struct DeviceContext {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;      // around the walk kernels
     cudaEvent_t ev_call0 = nullptr, ev_call1 = nullptr;    // around the whole call
+    cudaEvent_t ev_ref0 = nullptr, ev_ref1 = nullptr;      // around the refinement passes
+    void* list = nullptr;  // refinement work list (grow-only)
+    size_t list_bytes = 0;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
     void* pinned = nullptr;
@@ -30,6 +33,9 @@ DeviceContext* get_context(int device, int* st);
 
 // Ensures ctx->scratch holds at least `bytes` (grows, never shrinks).
 int ensure_scratch(DeviceContext* ctx, size_t bytes);
+
+// Ensures ctx->list holds at least `bytes` (grows, never shrinks).
+int ensure_list(DeviceContext* ctx, size_t bytes);
 
 // Ensures ctx->pinned holds at least `bytes` of page-locked host memory.
 int ensure_pinned(DeviceContext* ctx, size_t bytes);

@@ -85,6 +85,27 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
         pb.de_hi[pos] = s.hi;
         pb.de_lo[pos] = s.lo;
     }
+    // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
+    //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|.
+    __syncthreads();  // the complex bound reads the table written above
+    for (int r = tid; r < n; r += bd) {
+        if (c == 1) {
+            double lo = 0.0, hi = 0.0;
+            for (int j = 0; j < w; ++j) {
+                double v = pb.as[(size_t)r * n + j];
+                if (v < 0.0) lo += v; else hi += v;
+            }
+            pb.bnd[r] = lo;
+            pb.bnd[n + r] = hi;
+        } else {
+            double m = 0.0;
+            for (int d = 0; d < terms; ++d) {
+                size_t pos = ((size_t)(d / G) * n + r) * G + (d % G);
+                m = fmax(m, hypot(pb.de_hi[pos], pb.de_hi[(size_t)terms * n + pos]));
+            }
+            pb.bnd[r] = m * (1.0 + 0x1p-50);
+        }
+    }
     // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
     const int ntop = n - 1 - w;
     for (int idx = tid; idx < ntop * n * c; idx += bd) {
@@ -153,7 +174,15 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     size_t o_tick = take(sizeof(unsigned) * 4);
     size_t o_res = take(sizeof(dd) * 2);
     size_t o_exp = take(sizeof(int) * 4);
+    size_t o_bnd = take(sizeof(double) * 2 * n);
+    size_t o_hs = take(sizeof(double) * kHistBins);
+    size_t o_hc = take(sizeof(unsigned long long) * kHistBins);
+    size_t o_ln = take(sizeof(unsigned long long) * 2);
     if (base) {
+        pb->bnd = reinterpret_cast<double*>(base + o_bnd);
+        pb->hist_s2 = reinterpret_cast<double*>(base + o_hs);
+        pb->hist_cnt = reinterpret_cast<unsigned long long*>(base + o_hc);
+        pb->list_n = reinterpret_cast<unsigned long long*>(base + o_ln);
         pb->as = reinterpret_cast<double*>(base + o_as);
         pb->x0_hi = reinterpret_cast<double*>(base + o_x0h);
         pb->x0_lo = reinterpret_cast<double*>(base + o_x0l);
@@ -175,7 +204,37 @@ size_t walk_smem_bytes(const Problem& pb, int threads)
     size_t terms = (size_t)1 << pb.w;
     int ntop = n - 1 - pb.w;
     return sizeof(double) * (terms * n * c + (size_t)(ntop > 0 ? ntop : 0) * n * c +
-                             (size_t)n * c * threads);
+                             (size_t)n * c * threads) +
+           kHistSmemBytes;
+}
+
+// Picks the histogram bin (bins are keyed by each unit's bound U and hold the
+// units' actual sums of squared terms) from which units are re-evaluated in
+// double-double: the unrefined units' expected FP64 rounding error,
+// sqrt(sum t^2 * k/12) * 2^-52 with k rounded operations per term, must stay
+// below half the tolerance relative to the first-pass magnitude.  At most 1/8
+// of the units are refined; past that the estimate is reported instead.
+// Returns the bin; sets *count (units to refine) and *err_est.
+static int pick_threshold(const double* s2, const unsigned long long* cnt, int n, int comps,
+                          double mag, double tol, unsigned long long units,
+                          unsigned long long* count, double* err_est)
+{
+    const double k = comps == 1 ? 2.0 * n : 6.0 * n;
+    const double var_per_s2 = k / 12.0 * std::ldexp(1.0, -104);
+    const double budget = mag > 0.0 ? (0.5 * tol * mag) * (0.5 * tol * mag) : 0.0;
+    double cum = 0.0;
+    int b = 0;
+    while (b < kHistBins && cum + s2[b] * var_per_s2 <= budget) cum += s2[b++] * var_per_s2;
+    unsigned long long c = 0;
+    for (int i = b; i < kHistBins; ++i) c += cnt[i];
+    while (c > units / 8 && b < kHistBins) {
+        cum += s2[b] * var_per_s2;
+        c -= cnt[b];
+        ++b;
+    }
+    *count = c;
+    *err_est = mag > 0.0 ? std::sqrt(cum) / mag : INFINITY;
+    return b;
 }
 
 static int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in,
@@ -242,13 +301,20 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
                                      cudaMemcpyHostToDevice, stream));
         d_a = d_in;
     }
+    const bool dd_mode = opt.precision == SPB_PREC_DD;
+    pb.mode = dd_mode ? 1 : 0;
     SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
+    if (dd_mode) {
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_s2, 0, sizeof(double) * kHistBins, stream));
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_cnt, 0, sizeof(unsigned long long) * kHistBins, stream));
+    }
     setup_kernel<<<1, 512, 0, stream>>>(pb, d_a);
     SPB_CUDA_TRY(cudaGetLastError());
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
     st = launch_walk(pb, blocks, threads, smem, stream);
     if (st != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
+    int launches = 2;
 
     struct {
         dd res[2];
@@ -256,6 +322,53 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
     } h;
     SPB_CUDA_TRY(cudaMemcpyAsync(h.res, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
     SPB_CUDA_TRY(cudaMemcpyAsync(&h.e, pb.exp_sum, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    double ms_refine = 0.0;
+    if (dd_mode) {
+        // First pass done: read its total and the unit histogram.
+        static thread_local double hs2[kHistBins];
+        static thread_local unsigned long long hcnt[kHistBins];
+        SPB_CUDA_TRY(cudaMemcpyAsync(hs2, pb.hist_s2, sizeof(hs2), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaMemcpyAsync(hcnt, pb.hist_cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+        const double tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
+        const double mag = comps == 1 ? std::fabs(h.res[0].hi) : std::hypot(h.res[0].hi, h.res[1].hi);
+        unsigned long long count = 0;
+        double err = 0.0;
+        const int thr = pick_threshold(hs2, hcnt, n, comps, mag, tol, pb.units, &count, &err);
+        out->err_est = err;
+        if (count > 0) {
+            const size_t entry = sizeof(double) * 2 * n * comps;
+            if ((st = ensure_list(ctx, count * (entry + sizeof(unsigned long long)) + 256)) != SPB_OK)
+                return out->status = st;
+            pb.mode = 2;
+            pb.thr_bin = thr;
+            pb.list_cap = count;
+            pb.list_u = static_cast<unsigned long long*>(ctx->list);
+            pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
+                                                  align_up(count * sizeof(unsigned long long), 256));
+            SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
+            if ((st = launch_walk(pb, blocks, threads, smem, stream)) != SPB_OK) return out->status = st;
+            if ((st = launch_refine(pb, count, blocks, stream)) != SPB_OK) return out->status = st;
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref1, stream));
+            launches += 2;
+            dd corr[2];
+            unsigned long long listed = 0;
+            SPB_CUDA_TRY(cudaMemcpyAsync(corr, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
+            SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
+            SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+            if (listed != count) {
+                spb_set_error("refinement listed %llu units, histogram counted %llu",
+                              (unsigned long long)listed, (unsigned long long)count);
+                return out->status = SPB_ERR_CUDA;
+            }
+            for (int cc = 0; cc < comps; ++cc) h.res[cc] = dd_add(h.res[cc], corr[cc]);
+            float mr = 0.f;
+            SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
+            ms_refine = mr;
+            out->refined_units = count;
+        }
+    }
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
     SPB_CUDA_TRY(cudaStreamSynchronize(stream));
     float ms = 0.f, ms_call = 0.f;
@@ -271,10 +384,10 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
         out->imag = sgn * std::ldexp(h.res[1].hi, e);
         out->imag_lo = sgn * std::ldexp(h.res[1].lo, e);
     }
-    out->kernel_s = ms * 1e-3;
+    out->kernel_s = (ms + ms_refine) * 1e-3;
     out->device_s = ms_call * 1e-3;
     out->gray_steps = (uint64_t)n << (n - 1);
-    out->launches = 2;
+    out->launches = launches;
     out->status = SPB_OK;
     out->elapsed_s = wall_seconds() - t_start;
     return SPB_OK;

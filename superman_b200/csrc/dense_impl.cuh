@@ -26,7 +26,70 @@ struct Problem {
     unsigned* ticket;          // last-CTA election counter (reset by the kernel)
     dd* result;                // [comps] grid total
     int* exp_sum;              // sum of the row scaling exponents
+    // Double-double refinement (SPB_PREC_DD); unused when mode == 0.
+    int mode;                  // 0 walk, 1 walk + unit-bound histogram, 2 scan only
+    int thr_bin;               // mode 2: list the units whose bound bin >= thr_bin
+    double* bnd;               // real [2][n] min/max of DE over d; complex [n] max |DE|
+    double* hist_s2;           // [kHistBins] sum of squared terms of the units per bin
+    unsigned long long* hist_cnt;  // [kHistBins] units per bin
+    unsigned long long* list_n;    // mode 2: number of listed units
+    unsigned long long list_cap;
+    unsigned long long* list_u;    // [list_cap] unit index
+    double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
 };
+
+// Unit-bound histogram: bin = (ilogb(U) + 1024) / 4, i.e. four octaves per bin.
+constexpr int kHistBins = 512;
+
+__device__ __forceinline__ int hist_bin(double u)
+{
+    if (!(u > 0.0)) return 0;
+    if (!isfinite(u)) return kHistBins - 1;
+    int b = (ilogb(u) + 1024) >> 2;
+    return b < 0 ? 0 : (b >= kHistBins ? kHistBins - 1 : b);
+}
+
+// Shared memory the histogram needs (reserved in every mode so the walk and
+// the scan run with the same launch shape, hence the same unit split).
+constexpr size_t kHistSmemBytes = kHistBins * (sizeof(double) + sizeof(unsigned long long));
+
+// Per-thread cache of the histogram: consecutive Gray units of one thread
+// usually fall in the same bin, so shared-memory atomics are issued only when
+// the bin changes.
+struct HistCache {
+    int bin = -1;
+    double s2 = 0.0;
+    unsigned long long cnt = 0;
+    __device__ __forceinline__ void add(int b, double v, double* s_hist, unsigned long long* s_cnt)
+    {
+        if (b != bin) {
+            flush(s_hist, s_cnt);
+            bin = b;
+        }
+        s2 += v;
+        ++cnt;
+    }
+    __device__ __forceinline__ void flush(double* s_hist, unsigned long long* s_cnt)
+    {
+        if (cnt) {
+            atomicAdd(&s_hist[bin], s2);
+            atomicAdd(&s_cnt[bin], cnt);
+        }
+        s2 = 0.0;
+        cnt = 0;
+    }
+};
+
+// Flushes a CTA's shared histogram into the global one.
+__device__ __forceinline__ void flush_hist(const double* s_hist, const unsigned long long* s_cnt,
+                                           const Problem& pb)
+{
+    for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
+        if (s_cnt[i]) {
+            atomicAdd(&pb.hist_cnt[i], s_cnt[i]);
+            atomicAdd(&pb.hist_s2[i], s_hist[i]);
+        }
+}
 
 // Thread caps keep the x vector (2 registers per double) plus the product
 // chains under the per-thread register budget the cap implies
@@ -96,11 +159,13 @@ __device__ __forceinline__ void grid_reduce(dd (&tot)[C], const Problem& pb)
 
 // ---------------------------------------------------------------- real ----
 // Sum over one unit: sum_d (-1)^popc(d) prod_r (xh_r + DE[d][r]).
-template <int N, int G>
+// With STATS, also returns sum_d term_d^2 in *s2 (one FMA per term; sizes the
+// double-double refinement).
+template <int N, int G, bool STATS = false>
 __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const double* __restrict__ s_de,
-                                                int nq)
+                                                int nq, double* s2 = nullptr)
 {
-    double acc = 0.0;
+    double acc = 0.0, sq = 0.0;
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const double* de = s_de + q * (N * G);
@@ -135,7 +200,12 @@ __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const dou
         else if constexpr (G == 2) gs = sub_rn(p[0], p[1]);
         else gs = p[0];
         acc = (__popc(q) & 1) ? sub_rn(acc, gs) : add_rn(acc, gs);
+        if constexpr (STATS) {
+#pragma unroll
+            for (int i = 0; i < G; ++i) sq = __fma_rn(p[i], p[i], sq);
+        }
     }
+    if constexpr (STATS) *s2 = sq;
     return acc;
 }
 
@@ -152,8 +222,13 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     double* s_de = smem;
     double* s_mt = s_de + terms * N;
     double* s_lo = s_mt + (ntop > 0 ? ntop : 0) * N;
+    double* s_hist = s_lo + N * bd;  // mode 1
+    unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
     for (int i = tid; i < terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < ntop * N; i += bd) s_mt[i] = pb.mt[i];
+    const int mode = pb.mode;
+    if (mode == 1)
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
     __syncthreads();
 
     const unsigned long long T = (unsigned long long)gridDim.x * bd;
@@ -161,6 +236,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     unsigned long long u0, u1;
     balanced_range(pb.units, T, t, &u0, &u1);
     dd tot[1] = {{0.0, 0.0}};
+    HistCache hc;
     if (u0 < u1) {
         double xh[N];
         const unsigned long long g0 = gray_of(u0);
@@ -174,8 +250,34 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
         }
         unsigned long long u = u0;
         while (true) {
-            double us = unit_sum_real<N, G>(xh, s_de, nq);
-            tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
+            int b = 0;
+            if (mode != 0) {
+                // Upper bound of |term| over the unit: prod_r max |xh_r + DE[d][r]|;
+                // the scan recomputes it bit for bit to select the same units.
+                double ub = 1.0;
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+                    ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], pb.bnd[r])), fabs(add_rn(xh[r], pb.bnd[N + r]))));
+                b = hist_bin(ub);
+                if (mode == 2 && b >= pb.thr_bin) {
+                    unsigned long long k = atomicAdd(pb.list_n, 1ull);
+                    if (k < pb.list_cap) {
+                        pb.list_u[k] = u;
+                        double* dst = pb.list_x + k * (2 * N);
+#pragma unroll
+                        for (int r = 0; r < N; ++r) { dst[r] = xh[r]; dst[N + r] = s_lo[r * bd + tid]; }
+                    }
+                }
+            }
+            if (mode == 0) {
+                double us = unit_sum_real<N, G>(xh, s_de, nq);
+                tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
+            } else if (mode == 1) {
+                double sq;
+                double us = unit_sum_real<N, G, true>(xh, s_de, nq, &sq);
+                tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
+                hc.add(b, sq, s_hist, s_cnt);  // actual sum of squared terms, keyed by the bound
+            }
             if (++u >= u1) break;
             const int j = __ffsll((long long)u) - 1;
             const bool add = (gray_of(u) >> j) & 1ull;
@@ -190,17 +292,22 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
             }
         }
     }
-    grid_reduce<1>(tot, pb);
+    if (mode == 1) {
+        hc.flush(s_hist, s_cnt);
+        __syncthreads();
+        flush_hist(s_hist, s_cnt, pb);
+    }
+    if (mode != 2) grid_reduce<1>(tot, pb);
 }
 
 // ------------------------------------------------------------- complex ----
-template <int N, int G>
+template <int N, int G, bool STATS = false>
 __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const double (&xi)[N],
                                                  const double* __restrict__ s_de_re,
                                                  const double* __restrict__ s_de_im, int nq,
-                                                 double& acc_re, double& acc_im)
+                                                 double& acc_re, double& acc_im, double* s2 = nullptr)
 {
-    double ar = 0.0, ai = 0.0;
+    double ar = 0.0, ai = 0.0, sq = 0.0;
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const double* dr = s_de_re + q * (N * G);
@@ -239,9 +346,14 @@ __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const do
         else { gr = pr[0]; gi = pi[0]; }
         if (__popc(q) & 1) { ar = sub_rn(ar, gr); ai = sub_rn(ai, gi); }
         else { ar = add_rn(ar, gr); ai = add_rn(ai, gi); }
+        if constexpr (STATS) {
+#pragma unroll
+            for (int i = 0; i < G; ++i) sq = __fma_rn(pi[i], pi[i], __fma_rn(pr[i], pr[i], sq));
+        }
     }
     acc_re = ar;
     acc_im = ai;
+    if constexpr (STATS) *s2 = sq;
 }
 
 template <int N>
@@ -258,8 +370,13 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     double* s_de = smem;                        // [2][terms*N]
     double* s_mt = s_de + 2 * terms * N;        // [2][ntop*N]
     double* s_lo = s_mt + 2 * ntp * N;          // [2][N][bd]
+    double* s_hist = s_lo + 2 * N * bd;         // mode 1
+    unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
     for (int i = tid; i < 2 * terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < 2 * ntp * N; i += bd) s_mt[i] = pb.mt[i];
+    const int mode = pb.mode;
+    if (mode == 1)
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
     __syncthreads();
     const double* s_mt_re = s_mt;
     const double* s_mt_im = s_mt + ntp * N;
@@ -271,6 +388,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     unsigned long long u0, u1;
     balanced_range(pb.units, T, t, &u0, &u1);
     dd tot[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    HistCache hc;
     if (u0 < u1) {
         double xr[N], xi[N];
         const unsigned long long g0 = gray_of(u0);
@@ -290,11 +408,38 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
         }
         unsigned long long u = u0;
         while (true) {
-            double ur, ui;
-            unit_sum_complex<N, G>(xr, xi, s_de, s_de + terms * N, nq, ur, ui);
-            if (u & 1ull) { ur = -ur; ui = -ui; }
-            tot[0] = dd_add_d(tot[0], ur);
-            tot[1] = dd_add_d(tot[1], ui);
+            int b = 0;
+            if (mode != 0) {
+                // |x_r| <= |xtop_r| + max_d |DE[d][r]|  (triangle inequality)
+                double ub = 1.0;
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+                    ub = mul_rn(ub, add_rn(__dsqrt_rn(__fma_rn(xr[r], xr[r], mul_rn(xi[r], xi[r]))), pb.bnd[r]));
+                b = hist_bin(ub);
+                if (mode == 2 && b >= pb.thr_bin) {
+                    unsigned long long k = atomicAdd(pb.list_n, 1ull);
+                    if (k < pb.list_cap) {
+                        pb.list_u[k] = u;
+                        double* dst = pb.list_x + k * (4 * N);
+#pragma unroll
+                        for (int r = 0; r < N; ++r) {
+                            dst[r] = xr[r];
+                            dst[N + r] = s_lo_re[r * bd + tid];
+                            dst[2 * N + r] = xi[r];
+                            dst[3 * N + r] = s_lo_im[r * bd + tid];
+                        }
+                    }
+                }
+            }
+            if (mode != 2) {
+                double ur, ui, sq = 0.0;
+                if (mode == 0) unit_sum_complex<N, G>(xr, xi, s_de, s_de + terms * N, nq, ur, ui);
+                else unit_sum_complex<N, G, true>(xr, xi, s_de, s_de + terms * N, nq, ur, ui, &sq);
+                if (u & 1ull) { ur = -ur; ui = -ui; }
+                tot[0] = dd_add_d(tot[0], ur);
+                tot[1] = dd_add_d(tot[1], ui);
+                if (mode == 1) hc.add(b, sq, s_hist, s_cnt);
+            }
             if (++u >= u1) break;
             const int j = __ffsll((long long)u) - 1;
             const bool add = (gray_of(u) >> j) & 1ull;
@@ -313,8 +458,18 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
             }
         }
     }
-    grid_reduce<2>(tot, pb);
+    if (mode == 1) {
+        hc.flush(s_hist, s_cnt);
+        __syncthreads();
+        flush_hist(s_hist, s_cnt, pb);
+    }
+    if (mode != 2) grid_reduce<2>(tot, pb);
 }
+
+// Re-evaluates the units listed by a mode-2 scan in double-double and
+// accumulates (double-double unit sum - the walk's FP64 unit sum) into
+// pb.result, one warp per unit.  Defined in dense_refine.cu.
+int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s);
 
 // Per-n dispatch (defined in the instantiation units).
 int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
