@@ -114,6 +114,29 @@ SPB_API int spb_perm_dense_c128(const double* a, int n, const spb_options* opt, 
 SPB_API int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options* opt,
                             spb_result* out);
 
+/* Permanents of `count` n x n matrices in one launch, one warp per matrix
+ * (1 <= n <= 24).  d_mats: device, count consecutive row-major matrices
+ * (is_complex: interleaved re/im, 2*n*n doubles each); d_out: device,
+ * 2 doubles per component per matrix, the permanent as a double-double
+ * (hi, lo).  Asynchronous on `stream` (NULL = default stream); allocates
+ * nothing.  Batched counterpart of the dense drivers above for the many
+ * small permanents a serving queue or a decomposition produces; the
+ * reference runs each of them through its own chunk loop and launches
+ * (Algorithms/GPU/Dense/dpSingleGPU.cuh:156-199). */
+SPB_API int spb_perm_batch_dev(const double* d_mats, int n, int is_complex, int count,
+                               double* d_out, void* stream);
+
+/* Exact permanent of a 0/1 matrix (a: n*n bytes, row-major, nonzero = 1) by
+ * plain Ryser over all 2^n column subsets in wrap-around integer arithmetic
+ * whose width (128, 192 or 320 bits) is chosen from a Bregman-Minc bound, so
+ * the result is exact for every n <= 63.  limbs receives the permanent as a
+ * 320-bit two's-complement integer in ten little-endian 32-bit words;
+ * out->value is its nearest double.  Replaces the reference's 0/1 handling,
+ * which reads the pattern (IO/IO.h:441-443) and runs the FP64 dense path
+ * (Algorithms/GPU/Dense/dpSingleGPU.cuh:45-219), inexact beyond 2^53. */
+SPB_API int spb_perm_binary(const uint8_t* a, int n, const spb_options* opt, uint32_t* limbs,
+                            spb_result* out);
+
 /* Dense real permanent that allocates nothing, for callers that cannot let a
  * library call cudaMalloc/cudaFree: programs that reserve all device memory
  * for their own pool allocator, and latency-bound request loops that cannot
@@ -128,6 +151,58 @@ SPB_API int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options*
  * No counterpart in the reference, which allocates on every call
  * (Algorithms/GPU/Dense/dpSingleGPU.cuh:138-144). */
 SPB_API int spb_perm_dense_f64_noalloc(const double* d_a, int n, double* d_out, void* stream);
+
+/* ------------------------------------------------ host pipeline ---- */
+
+/* Outcome of the reference's top-level flow (main.cpp:42-151). */
+typedef struct spb_pipeline_result {
+    double permanent;  /* real permanent, or the real part                   */
+    double imag;       /* imaginary part (complex=true)                      */
+    double time_s;     /* the reference's "Computed in" time                 */
+    double avg_n;      /* mean size of the decomposed pieces ("Average N")   */
+    double avg_nnz;    /* mean nonzeros of the pieces ("Average NNZ")        */
+    int components;    /* bipartite connected components after pruning       */
+    int pieces;        /* pieces computed ("Submatrix count")                */
+    int algorithm;     /* Algorithm enum value chosen (Settings.h)           */
+    int status;
+} spb_pipeline_result;
+
+/* Runs main.cpp's real-matrix flow on an in-memory row-major matrix:
+ * perfect-matching pruning (IO/IO.h:477-508, IO/dm.cpp:441-501), connected
+ * components (IO/dm.h:43-107), AlgorithmSelector (CommonFiles/
+ * AlgorithmSelector.h:49-141), DecomposePerman (CommonFiles/
+ * DecomposePerman.h:76-557) and the GPU drivers, with settings given as the
+ * reference's key=value arguments (IO/IO.h:163-401), e.g. "algorithm=auto",
+ * "calculation_precision=dd", "binary=true", "scaling=true".  mode=cpu and
+ * the multi-GPU modes are reported as unavailable (SPB_ERR_INVALID). */
+SPB_API int spb_perm_pipeline(const double* a, int n, const char* const* args, int nargs,
+                              spb_pipeline_result* out);
+
+/* The whole reference program on a matrix file: args as on its command line
+ * ("filename=...", "complex=true", "binary=true", "undirected=true", ...);
+ * replaces main.cpp:42-151 with IO::readMatrix / IO::readComplex
+ * (IO/IO.h:403-596). */
+SPB_API int spb_perm_file(const char* const* args, int nargs, spb_pipeline_result* out);
+
+/* Reads a matrix file as IO::readMatrix / IO::readComplex do (IO/IO.h:403-596),
+ * pruning included for real matrices.  *n is always set; the entries are
+ * copied to `out` (row-major; interleaved re/im when is_complex) when out is
+ * non-null and n <= max_n.  CPU only. */
+SPB_API int spb_read_matrix(const char* path, int binary, int undirected, int is_complex, double* out,
+                            int max_n, int* n, double* sparsity);
+
+/* Perfect-matching pruning of a dense row-major matrix into out (n*n); sets
+ * *has_perfect_matching (0: the permanent is structurally zero and out is
+ * all zeros).  Replaces dm() (IO/dm.cpp:441-501).  CPU only. */
+SPB_API int spb_dm_prune(const double* a, int n, double* out, int* has_perfect_matching);
+
+/* The pieces DecomposePerman (CommonFiles/DecomposePerman.h:120-198) would
+ * compute for a matrix, without computing them: *count pieces, sizes[k] and
+ * their row-major entries concatenated in data.  Pass sizes = data = NULL to
+ * query *count alone.  The permanents of the pieces sum to the permanent of
+ * the matrix.  CPU only. */
+SPB_API int spb_decompose(const double* a, int n, int* count, int* sizes, double* data, int max_pieces,
+                          size_t max_doubles);
 
 /* Measured pipe throughput used as the roofline denominator: which = 0 gives
  * FP64 FMA thread-instructions per second, which = 1 gives int32 multiply-add

@@ -197,6 +197,30 @@ def exact_perm(a, threads=None) -> Fraction:
     return Fraction(val, 1 << shift)
 
 
+def exact_perm_fractions(a, threads=None) -> Fraction:
+    """Exact permanent of a matrix of Fractions (or ints): each row is scaled
+    by the lcm of its denominators, the integer permanent found by CRT."""
+    n = len(a)
+    if n == 0:
+        return Fraction(1)
+    K, scale = [], 1
+    for row in a:
+        row = [Fraction(v) for v in row]
+        den = 1
+        for v in row:
+            den = den * v.denominator // math.gcd(den, v.denominator)
+        scale *= den
+        K.append([int(v * den) for v in row])
+    bound_bits = sum(max(1, sum(abs(v) for v in row)).bit_length() for row in K) + 1
+    primes = _primes_for(bound_bits)
+    kmod = np.array([[[v % p for v in row] for row in K] for p in primes], dtype=np.uint64)
+    pr = np.array(primes, dtype=np.uint64)
+    out = np.zeros(len(primes), dtype=np.uint64)
+    lib().orc_perm_mod_primes(_u64ptr(kmod), n, _u64ptr(pr), len(primes), _threads(threads),
+                              _u64ptr(out))
+    return Fraction(_crt_signed([int(v) for v in out], primes), scale)
+
+
 def exact_perm_complex(a, threads=None):
     """Exact (re, im) permanent of a complex128 matrix, as two Fractions."""
     a = np.asarray(a, dtype=np.complex128)

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
 
-__all__ = ["Result", "perm_dense", "perm_complex", "SupermanError", "SPB_PREC_FP64",
+__all__ = ["Result", "perm_dense", "perm_complex", "perm_binary", "SupermanError", "SPB_PREC_FP64",
            "SPB_PREC_DD", "device_count"]
 
 _PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD}
@@ -65,6 +65,28 @@ def perm_dense(a, precision="fp64", device: int = 0, **shape) -> Result:
                                        a.shape[0], ctypes.byref(opt), ctypes.byref(out))
     _lib.check(st)
     return _to_result(out, False)
+
+
+def perm_binary(a, device: int = 0, **shape) -> Result:
+    """Exact permanent of a 0/1 n x n matrix (1 <= n <= 63); Result.permanent
+    is a Python int."""
+    a = np.ascontiguousarray(np.asarray(a) != 0, dtype=np.uint8)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("perm_binary needs a square 2-D array")
+    out = _lib.spb_result()
+    limbs = (ctypes.c_uint32 * 10)()
+    opt = _lib.default_options(device=device, **shape)
+    st = _lib.lib().spb_perm_binary(a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), a.shape[0],
+                                    ctypes.byref(opt), limbs, ctypes.byref(out))
+    _lib.check(st)
+    v = 0
+    for i in reversed(range(10)):
+        v = (v << 32) | limbs[i]
+    if v >> 319:
+        v -= 1 << 320
+    res = _to_result(out, False)
+    res.permanent = v
+    return res
 
 
 def perm_complex(a, precision="fp64", device: int = 0, **shape) -> Result:

@@ -68,6 +68,20 @@ class spb_result(ctypes.Structure):
     ]
 
 
+class spb_pipeline_result(ctypes.Structure):
+    _fields_ = [
+        ("permanent", ctypes.c_double),
+        ("imag", ctypes.c_double),
+        ("time_s", ctypes.c_double),
+        ("avg_n", ctypes.c_double),
+        ("avg_nnz", ctypes.c_double),
+        ("components", ctypes.c_int),
+        ("pieces", ctypes.c_int),
+        ("algorithm", ctypes.c_int),
+        ("status", ctypes.c_int),
+    ]
+
+
 _DP = ctypes.POINTER(ctypes.c_double)
 _OP = ctypes.POINTER(spb_options)
 _RP = ctypes.POINTER(spb_result)
@@ -83,8 +97,21 @@ SIGNATURES = {
     "spb_perm_dense_f64_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128": (ctypes.c_int, [_DP, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),
+    "spb_perm_batch_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
+    "spb_perm_binary": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint8), ctypes.c_int, _OP,
+                                       ctypes.POINTER(ctypes.c_uint32), _RP]),
     "spb_perm_dense_f64_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                   ctypes.c_void_p]),
+    "spb_perm_pipeline": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                                         ctypes.POINTER(spb_pipeline_result)]),
+    "spb_perm_file": (ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                                     ctypes.POINTER(spb_pipeline_result)]),
+    "spb_read_matrix": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP,
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP]),
+    "spb_dm_prune": (ctypes.c_int, [_DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int)]),
+    "spb_decompose": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), _DP, ctypes.c_int, ctypes.c_size_t]),
     "spb_measure_pipe_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_double)]),
 }

@@ -1,0 +1,206 @@
+// Many small permanents in one launch: one warp per matrix.
+//
+// The whole-GPU walk (dense_impl.cuh) spreads one permanent over every SM;
+// for n <= 24 a permanent is too small for that (2^(n-1) terms, a few
+// microseconds of FP64 work) and launch latency dominates.  Here each warp
+// takes a matrix of the batch (grid-stride over the batch), builds its row
+// scaling, double-double NW start vector, low-column subset-sum table and
+// high columns in the warp's slice of shared memory, then its 32 lanes split
+// the Gray units of that matrix exactly as the threads of the big walk do
+// (same unit evaluators; the double-double unit bases live in registers), and
+// a warp reduction gives the double-double total.  The permanent of matrix m
+// is written as (hi, lo) per component: out[m*2*comps + 2*c + {0, 1}].
+//
+// Device pointers only, no allocation, no host synchronisation: the serving
+// loop captures one launch per batch shape in a CUDA graph, and the
+// decomposition path runs its independent pieces through it.
+#include <cuda_runtime.h>
+
+#include "dense_impl.cuh"
+#include "spb_common.cuh"
+
+namespace spb {
+namespace batch {
+
+constexpr int kMaxN = 24;
+constexpr int kWarpsPerCta = 4;
+
+template <int N, int C>
+struct Cfg {
+    static constexpr int W = (N - 1) < 5 ? (N - 1) : 5;  // low column bits per unit
+    static constexpr int G = C == 1 ? (W >= 2 ? 4 : (W == 1 ? 2 : 1)) : (W >= 1 ? 2 : 1);
+    static constexpr int TERMS = 1 << W;
+    static constexpr int NTOP = N - 1 - W;
+    static constexpr int NTP = NTOP > 0 ? NTOP : 0;
+    // doubles per warp: DE table, high columns, x0 hi/lo, row exponents (as doubles)
+    static constexpr int SMEM_DOUBLES = TERMS * N * C + NTP * N * C + 2 * N * C + N;
+};
+
+template <int N, int C>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __restrict__ mats,
+                                                                 int count, double* __restrict__ out)
+{
+    using Q = Cfg<N, C>;
+    constexpr int G = Q::G, TERMS = Q::TERMS, NTOP = Q::NTOP, NTP = Q::NTP, W = Q::W;
+    extern __shared__ __align__(16) double smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* s_de = smem + (size_t)wid * Q::SMEM_DOUBLES;  // [C][TERMS/G][N][G]
+    double* s_mt = s_de + TERMS * N * C;                  // [C][NTOP][N]
+    double* s_x0h = s_mt + NTP * N * C;                   // [C][N]
+    double* s_x0l = s_x0h + N * C;                        // [C][N]
+    int* s_exp = reinterpret_cast<int*>(s_x0l + N * C);   // [N]
+
+    const int total_warps = gridDim.x * kWarpsPerCta;
+    for (int m = blockIdx.x * kWarpsPerCta + wid; m < count; m += total_warps) {
+        const double* A = mats + (size_t)m * N * N * C;
+        // row exponents: row max scaled into [0.5, 1)
+        for (int r = lane; r < N; r += 32) {
+            double mx = 0.0;
+            for (int j = 0; j < N * C; ++j) mx = fmax(mx, fabs(A[r * N * C + j]));
+            int e = 0;
+            if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+            s_exp[r] = e;
+        }
+        __syncwarp();
+        // NW start vector (double-double)
+        for (int rr = lane; rr < N * C; rr += 32) {
+            const int r = rr / C, part = rr % C;
+            dd s = {0.0, 0.0};
+            for (int j = 0; j < N; ++j) s = dd_add_d(s, ldexp(A[(r * N + j) * C + part], -s_exp[r]));
+            dd h = {-0.5 * s.hi, -0.5 * s.lo};
+            dd x = dd_add_d(h, ldexp(A[(r * N + (N - 1)) * C + part], -s_exp[r]));
+            s_x0h[part * N + r] = x.hi;
+            s_x0l[part * N + r] = x.lo;
+        }
+        // low-column subset sums, grouped [part][d/G][r][d%G]
+        for (int idx = lane; idx < TERMS * N * C; idx += 32) {
+            const int part = idx / (TERMS * N), rem = idx % (TERMS * N);
+            const int d = rem / N, r = rem % N;
+            dd s = {0.0, 0.0};
+            for (int j = 0; j < W; ++j)
+                if ((d >> j) & 1) s = dd_add_d(s, ldexp(A[(r * N + j) * C + part], -s_exp[r]));
+            s_de[part * TERMS * N + ((d / G) * N + r) * G + (d % G)] = s.hi;
+        }
+        // high columns [part][j][r]
+        for (int idx = lane; idx < NTP * N * C; idx += 32) {
+            const int part = idx / (NTP * N), rem = idx % (NTP * N);
+            const int j = rem / N, r = rem % N;
+            s_mt[idx] = ldexp(A[(r * N + (W + j)) * C + part], -s_exp[r]);
+            (void)part;
+        }
+        __syncwarp();
+
+        unsigned long long u0, u1;
+        balanced_range(1ull << NTP, 32, lane, &u0, &u1);
+        dd tot[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) tot[c] = {0.0, 0.0};
+        if (u0 < u1) {
+            double xh[C][N], xl[C][N];
+            const unsigned long long g0 = gray_of(u0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+#pragma unroll
+                for (int r = 0; r < N; ++r) {
+                    dd x = {s_x0h[c * N + r], s_x0l[c * N + r]};
+                    for (int j = 0; j < NTOP; ++j)
+                        if ((g0 >> j) & 1ull) x = dd_add_d(x, s_mt[c * NTP * N + j * N + r]);
+                    xh[c][r] = x.hi;
+                    xl[c][r] = x.lo;
+                }
+            unsigned long long u = u0;
+            while (true) {
+                if constexpr (C == 1) {
+                    double us = dense::unit_sum_real<N, G>(xh[0], s_de, TERMS / G);
+                    tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
+                } else {
+                    double ur, ui;
+                    dense::unit_sum_complex<N, G>(xh[0], xh[C - 1], s_de, s_de + TERMS * N, TERMS / G, ur, ui);
+                    if (u & 1ull) { ur = -ur; ui = -ui; }
+                    tot[0] = dd_add_d(tot[0], ur);
+                    tot[C - 1] = dd_add_d(tot[C - 1], ui);
+                }
+                if (++u >= u1) break;
+                const int j = __ffsll((long long)u) - 1;
+                const bool add = (gray_of(u) >> j) & 1ull;
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+#pragma unroll
+                    for (int r = 0; r < N; ++r) {
+                        const double v = s_mt[c * NTP * N + j * N + r];
+                        dd s = two_sum(xh[c][r], add ? v : -v);
+                        dd z = fast_two_sum(s.hi, add_rn(s.lo, xl[c][r]));
+                        xh[c][r] = z.hi;
+                        xl[c][r] = z.lo;
+                    }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) tot[c] = warp_sum_dd(tot[c]);
+        if (lane == 0) {
+            int es = 0;
+            for (int r = 0; r < N; ++r) es += s_exp[r];
+            const double sgn = (N % 2) ? 1.0 : -1.0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                out[(size_t)m * 2 * C + 2 * c] = sgn * ldexp(tot[c].hi, es + 1);
+                out[(size_t)m * 2 * C + 2 * c + 1] = sgn * ldexp(tot[c].lo, es + 1);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int N, int C>
+int launch_n(const double* mats, int count, double* out, int sms, cudaStream_t s)
+{
+    constexpr size_t smem = sizeof(double) * Cfg<N, C>::SMEM_DOUBLES * kWarpsPerCta;
+    if (smem > 48 * 1024) {
+        static cudaError_t attr = cudaFuncSetAttribute(batch_walk<N, C>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        SPB_CUDA_TRY(attr);
+    }
+    int blocks = (count + kWarpsPerCta - 1) / kWarpsPerCta;
+    const int cap = sms * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    batch_walk<N, C><<<blocks, kWarpsPerCta * 32, smem, s>>>(mats, count, out);
+    SPB_CUDA_TRY(cudaGetLastError());
+    return SPB_OK;
+}
+
+}  // namespace batch
+}  // namespace spb
+
+extern "C" int spb_perm_batch_dev(const double* d_mats, int n, int is_complex, int count, double* d_out,
+                                  void* stream)
+{
+    using namespace spb::batch;
+    if (!d_mats || !d_out || count < 0) {
+        spb_set_error("spb_perm_batch_dev: null pointer or negative count");
+        return SPB_ERR_INVALID;
+    }
+    if (n < 1 || n > kMaxN) {
+        spb_set_error("spb_perm_batch_dev: n=%d outside 1..%d (larger n: the whole-GPU entry points)", n, kMaxN);
+        return SPB_ERR_INVALID;
+    }
+    if (count == 0) return SPB_OK;
+    int dev = 0, sms = 0;
+    SPB_CUDA_TRY(cudaGetDevice(&dev));
+    SPB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int key = n * 2 + (is_complex ? 1 : 0);
+    switch (key) {
+#define SPB_BCASE(N)                                                    \
+    case 2 * N: return launch_n<N, 1>(d_mats, count, d_out, sms, s);    \
+    case 2 * N + 1: return launch_n<N, 2>(d_mats, count, d_out, sms, s);
+        SPB_BCASE(1) SPB_BCASE(2) SPB_BCASE(3) SPB_BCASE(4) SPB_BCASE(5) SPB_BCASE(6) SPB_BCASE(7)
+        SPB_BCASE(8) SPB_BCASE(9) SPB_BCASE(10) SPB_BCASE(11) SPB_BCASE(12) SPB_BCASE(13)
+        SPB_BCASE(14) SPB_BCASE(15) SPB_BCASE(16) SPB_BCASE(17) SPB_BCASE(18) SPB_BCASE(19)
+        SPB_BCASE(20) SPB_BCASE(21) SPB_BCASE(22) SPB_BCASE(23) SPB_BCASE(24)
+#undef SPB_BCASE
+    default:
+        spb_set_error("spb_perm_batch_dev: unsupported n=%d", n);
+        return SPB_ERR_INVALID;
+    }
+}

@@ -1,0 +1,246 @@
+// Exact 0/1 permanent: plain Ryser over all 2^n column subsets,
+//   perm(A) = (-1)^n sum_S (-1)^|S| prod_r x_r(S),   x_r(S) = sum_{j in S} a_rj,
+// in wrap-around integer arithmetic modulo 2^(32L).  The host picks L from a
+// Bregman-Minc bound so that |perm| < 2^(32L-1): the result is then exact.
+//
+// The reference has no integer path: 0/1 input goes through its FP64 NW
+// walk (IO/IO.h:441-443 feeding Algorithms/GPU/Dense/dpSingleGPU.cuh), whose
+// result is off by ~1e-10 relative at n=30.
+//
+// Layout mirrors the dense walk: the w low columns are enumerated from a
+// shared table DEI[d][r] = number of ones of row r among the columns of d
+// (grouped [d/4][r][d%4], so one 16-byte broadcast load serves four terms);
+// the n-w high columns form a unit index walked in Gray order per thread with
+// the integer unit base xtop_r in registers.  Each term multiplies up to K
+// row sums in 32 bits (n^K < 2^32), then folds those partial products into L
+// 32-bit limbs with 32x32->64 multiply-adds.  Unit sums and the grid
+// reduction are exact, so the result does not depend on the launch shape.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "spb_common.cuh"
+
+namespace spb {
+namespace binary {
+
+constexpr int kMaxN = 63;
+constexpr int kMaxLimbs = 10;
+
+struct Problem {
+    int n, w, limbs, grid;
+    unsigned long long units;  // 2^(n-w) Gray units of 2^w terms each
+    const int* dei;            // [2^w/4][n][4] low-column row counts
+    const int8_t* mt;          // [n-w][n] high columns (0/1)
+    uint32_t* partials;        // [grid][limbs]
+    unsigned* ticket;          // last-CTA election (reset by the kernel)
+    uint32_t* result;          // [limbs] sum over subsets, mod 2^(32*limbs)
+};
+
+// Rows per 32-bit partial product: largest K with N^K < 2^32.
+__host__ __device__ constexpr int rows_per_word(int n)
+{
+    int k = 1;
+    unsigned long long p = (unsigned long long)(n > 1 ? n : 2);
+    while (p * (unsigned long long)(n > 1 ? n : 2) < (1ull << 32) && k < 16) {
+        p *= (unsigned long long)(n > 1 ? n : 2);
+        ++k;
+    }
+    return k;
+}
+
+template <int L>
+__device__ __forceinline__ void limb_add(uint32_t (&a)[L], const uint32_t (&b)[L])
+{
+    uint64_t c = 0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        uint64_t t = (uint64_t)a[i] + b[i] + c;
+        a[i] = (uint32_t)t;
+        c = t >> 32;
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void limb_sub(uint32_t (&a)[L], const uint32_t (&b)[L])
+{
+    uint64_t br = 0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        uint64_t t = (uint64_t)a[i] - b[i] - br;
+        a[i] = (uint32_t)t;
+        br = (t >> 63) & 1ull;
+    }
+}
+
+// prod_r x_r mod 2^(32L) for one term; x_r = xt[r] + de(r).
+template <int N, int L, int G>
+__device__ __forceinline__ void term_product(const int (&xt)[N], const int* __restrict__ de, int i,
+                                             uint32_t (&p)[L])
+{
+    constexpr int K = rows_per_word(N);
+    constexpr int NG = (N + K - 1) / K;
+#pragma unroll
+    for (int l = 0; l < L; ++l) p[l] = 0u;
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+        uint32_t w = 1u;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int r = g * K + k;
+            if (r < N) w *= (uint32_t)(xt[r] + de[r * G + i]);
+        }
+        if (g == 0) {
+            p[0] = w;
+        } else {
+            // p *= w, only the limbs that can be nonzero after g words
+            uint64_t c = 0;
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+                if (l <= g) {
+                    uint64_t t = (uint64_t)p[l] * w + c;
+                    p[l] = (uint32_t)t;
+                    c = t >> 32;
+                }
+            }
+        }
+    }
+}
+
+// Sum over one unit: sum_d (-1)^popc(d) prod_r (xt_r + DEI[d][r]).
+template <int N, int L>
+__device__ __forceinline__ void unit_sum_bin(const int (&xt)[N], const int* __restrict__ s_de, int nq,
+                                             uint32_t (&acc)[L])
+{
+    constexpr int G = 4;
+#pragma unroll
+    for (int l = 0; l < L; ++l) acc[l] = 0u;
+#pragma unroll 1
+    for (int q = 0; q < nq; ++q) {
+        const int* de = s_de + q * (N * G);
+        uint32_t p0[L], p1[L], p2[L], p3[L];
+        term_product<N, L, G>(xt, de, 0, p0);
+        term_product<N, L, G>(xt, de, 1, p1);
+        term_product<N, L, G>(xt, de, 2, p2);
+        term_product<N, L, G>(xt, de, 3, p3);
+        // group signs relative to popc(q): + - - +
+        limb_add<L>(p0, p3);
+        limb_add<L>(p1, p2);
+        if (__popc(q) & 1) {
+            limb_sub<L>(acc, p0);
+            limb_add<L>(acc, p1);
+        } else {
+            limb_add<L>(acc, p0);
+            limb_sub<L>(acc, p1);
+        }
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void shfl_add(uint32_t (&v)[L], int m)
+{
+    uint32_t o[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) o[l] = __shfl_xor_sync(0xffffffffu, v[l], m);
+    limb_add<L>(v, o);
+}
+
+// Threads per CTA: 512 keeps n <= 36 spill-free within 128 registers; larger
+// n (wider products, more limbs) gets 255 registers at 256 threads.
+__host__ __device__ constexpr int bin_max_threads(int n) { return n <= 36 ? 512 : 256; }
+
+template <int N, int L>
+__global__ void __launch_bounds__(bin_max_threads(N), 1) walk_binary(Problem pb)
+{
+    constexpr int G = 4;
+    extern __shared__ __align__(16) int smem_i[];
+    const int w = pb.w, terms = 1 << w, nq = terms / G, ntop = N - w;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    int* s_de = smem_i;
+    int8_t* s_mt = reinterpret_cast<int8_t*>(s_de + terms * N);
+    for (int i = tid; i < terms * N; i += bd) s_de[i] = pb.dei[i];
+    for (int i = tid; i < ntop * N; i += bd) s_mt[i] = pb.mt[i];
+    __syncthreads();
+
+    const unsigned long long T = (unsigned long long)gridDim.x * bd;
+    const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
+    unsigned long long u0, u1;
+    balanced_range(pb.units, T, t, &u0, &u1);
+    uint32_t tot[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) tot[l] = 0u;
+    if (u0 < u1) {
+        int xt[N];
+        const unsigned long long g0 = gray_of(u0);
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            int x = 0;
+            for (int j = 0; j < ntop; ++j)
+                if ((g0 >> j) & 1ull) x += s_mt[j * N + r];
+            xt[r] = x;
+        }
+        unsigned long long u = u0;
+        while (true) {
+            uint32_t us[L];
+            unit_sum_bin<N, L>(xt, s_de, nq, us);
+            if (u & 1ull) limb_sub<L>(tot, us);
+            else limb_add<L>(tot, us);
+            if (++u >= u1) break;
+            const int j = __ffsll((long long)u) - 1;
+            const int sg = ((gray_of(u) >> j) & 1ull) ? 1 : -1;
+            const int8_t* col = s_mt + j * N;
+#pragma unroll
+            for (int r = 0; r < N; ++r) xt[r] += sg * col[r];
+        }
+    }
+    // warp -> block -> grid (exact; order only affects speed)
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) shfl_add<L>(tot, m);
+    __shared__ uint32_t s_warp[16][kMaxLimbs];
+    __shared__ int s_last;
+    const int lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int l = 0; l < L; ++l) s_warp[wid][l] = tot[l];
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t v[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[l] = lane < nw ? s_warp[lane][l] : 0u;
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) shfl_add<L>(v, m);
+        if (lane == 0) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) pb.partials[blockIdx.x * L + l] = v[l];
+            __threadfence();
+            unsigned prev = atomicAdd(pb.ticket, 1u);
+            s_last = (prev == gridDim.x - 1) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    if (s_last && wid == 0) {
+        __threadfence();
+        uint32_t v[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[l] = 0u;
+        for (int b = lane; b < (int)gridDim.x; b += 32) {
+            uint32_t o[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) o[l] = __ldcg(pb.partials + b * L + l);
+            limb_add<L>(v, o);
+        }
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) shfl_add<L>(v, m);
+        if (lane == 0) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) pb.result[l] = v[l];
+            *pb.ticket = 0u;
+        }
+    }
+}
+
+int launch_binary(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+
+}  // namespace binary
+}  // namespace spb

@@ -178,7 +178,9 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     size_t o_hs = take(sizeof(double) * kHistBins);
     size_t o_hc = take(sizeof(unsigned long long) * kHistBins);
     size_t o_ln = take(sizeof(unsigned long long) * 2);
+    size_t o_tm = pb->mode != 0 ? take(sizeof(unsigned short) * (size_t)pb->grid * pb->threads) : 0;
     if (base) {
+        pb->tmax = pb->mode != 0 ? reinterpret_cast<unsigned short*>(base + o_tm) : nullptr;
         pb->bnd = reinterpret_cast<double*>(base + o_bnd);
         pb->hist_s2 = reinterpret_cast<double*>(base + o_hs);
         pb->hist_cnt = reinterpret_cast<unsigned long long*>(base + o_hc);
@@ -205,7 +207,7 @@ size_t walk_smem_bytes(const Problem& pb, int threads)
     int ntop = n - 1 - pb.w;
     return sizeof(double) * (terms * n * c + (size_t)(ntop > 0 ? ntop : 0) * n * c +
                              (size_t)n * c * threads) +
-           kHistSmemBytes;
+           kHistSmemBytes + bound_smem_bytes(n);
 }
 
 // Picks the histogram bin (bins are keyed by each unit's bound U and hold the
@@ -287,6 +289,9 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
     if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
     if (blocks < 1) blocks = 1;
     pb.grid = blocks;
+    pb.threads = threads;
+    const bool dd_mode = opt.precision == SPB_PREC_DD;
+    pb.mode = dd_mode ? 1 : 0;
 
     size_t in_off = 0;
     size_t need = plan_layout(&pb, nullptr, &in_off);
@@ -301,8 +306,6 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
                                      cudaMemcpyHostToDevice, stream));
         d_a = d_in;
     }
-    const bool dd_mode = opt.precision == SPB_PREC_DD;
-    pb.mode = dd_mode ? 1 : 0;
     SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
     if (dd_mode) {
         SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_s2, 0, sizeof(double) * kHistBins, stream));

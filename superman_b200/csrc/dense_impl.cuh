@@ -14,7 +14,7 @@ constexpr int kMaxN = 63;
 // Device-side description of one permanent: sizes plus pointers into the
 // scratch arena written by setup_kernel.
 struct Problem {
-    int n, comps, w, g, grid;
+    int n, comps, w, g, grid, threads;
     unsigned long long units;  // 2^(n-1-w) Gray units of 2^w terms each
     double* as;                // row-scaled matrix (row-major, comps interleaved)
     double* x0_hi;             // [comps][n] NW start vector, double-double
@@ -36,6 +36,7 @@ struct Problem {
     unsigned long long list_cap;
     unsigned long long* list_u;    // [list_cap] unit index
     double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
+    unsigned short* tmax;          // [grid*threads] highest bound bin of each thread's units
 };
 
 // Unit-bound histogram: bin = (ilogb(U) + 1024) / 4, i.e. four octaves per bin.
@@ -52,6 +53,8 @@ __device__ __forceinline__ int hist_bin(double u)
 // Shared memory the histogram needs (reserved in every mode so the walk and
 // the scan run with the same launch shape, hence the same unit split).
 constexpr size_t kHistSmemBytes = kHistBins * (sizeof(double) + sizeof(unsigned long long));
+// Shared memory for the per-row bound terms (two per row, real or complex).
+__host__ __device__ constexpr size_t bound_smem_bytes(int n) { return sizeof(double) * 2 * n; }
 
 // Per-thread cache of the histogram: consecutive Gray units of one thread
 // usually fall in the same bin, so shared-memory atomics are issued only when
@@ -165,7 +168,9 @@ template <int N, int G, bool STATS = false>
 __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const double* __restrict__ s_de,
                                                 int nq, double* s2 = nullptr)
 {
-    double acc = 0.0, sq = 0.0;
+    double acc = 0.0, sq[G];
+#pragma unroll
+    for (int i = 0; i < G; ++i) sq[i] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const double* de = s_de + q * (N * G);
@@ -202,10 +207,15 @@ __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const dou
         acc = (__popc(q) & 1) ? sub_rn(acc, gs) : add_rn(acc, gs);
         if constexpr (STATS) {
 #pragma unroll
-            for (int i = 0; i < G; ++i) sq = __fma_rn(p[i], p[i], sq);
+            for (int i = 0; i < G; ++i) sq[i] = __fma_rn(p[i], p[i], sq[i]);
         }
     }
-    if constexpr (STATS) *s2 = sq;
+    if constexpr (STATS) {
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < G; ++i) t += sq[i];
+        *s2 = t;
+    }
     return acc;
 }
 
@@ -224,9 +234,12 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     double* s_lo = s_mt + (ntop > 0 ? ntop : 0) * N;
     double* s_hist = s_lo + N * bd;  // mode 1
     unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
+    double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);  // [2][N]
     for (int i = tid; i < terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < ntop * N; i += bd) s_mt[i] = pb.mt[i];
     const int mode = pb.mode;
+    if (mode != 0)
+        for (int i = tid; i < 2 * N; i += bd) s_bnd[i] = pb.bnd[i];
     if (mode == 1)
         for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
     __syncthreads();
@@ -235,8 +248,11 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
     unsigned long long u0, u1;
     balanced_range(pb.units, T, t, &u0, &u1);
+    // The scan only walks threads that own a unit at or above the threshold.
+    if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[1] = {{0.0, 0.0}};
     HistCache hc;
+    int bmax = 0;
     if (u0 < u1) {
         double xh[N];
         const unsigned long long g0 = gray_of(u0);
@@ -257,8 +273,9 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
                 double ub = 1.0;
 #pragma unroll
                 for (int r = 0; r < N; ++r)
-                    ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], pb.bnd[r])), fabs(add_rn(xh[r], pb.bnd[N + r]))));
+                    ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
                 b = hist_bin(ub);
+                bmax = b > bmax ? b : bmax;
                 if (mode == 2 && b >= pb.thr_bin) {
                     unsigned long long k = atomicAdd(pb.list_n, 1ull);
                     if (k < pb.list_cap) {
@@ -293,6 +310,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
         }
     }
     if (mode == 1) {
+        pb.tmax[t] = (unsigned short)bmax;
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
@@ -307,7 +325,9 @@ __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const do
                                                  const double* __restrict__ s_de_im, int nq,
                                                  double& acc_re, double& acc_im, double* s2 = nullptr)
 {
-    double ar = 0.0, ai = 0.0, sq = 0.0;
+    double ar = 0.0, ai = 0.0, sq[G];
+#pragma unroll
+    for (int i = 0; i < G; ++i) sq[i] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const double* dr = s_de_re + q * (N * G);
@@ -348,12 +368,17 @@ __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const do
         else { ar = add_rn(ar, gr); ai = add_rn(ai, gi); }
         if constexpr (STATS) {
 #pragma unroll
-            for (int i = 0; i < G; ++i) sq = __fma_rn(pi[i], pi[i], __fma_rn(pr[i], pr[i], sq));
+            for (int i = 0; i < G; ++i) sq[i] = __fma_rn(pi[i], pi[i], __fma_rn(pr[i], pr[i], sq[i]));
         }
     }
     acc_re = ar;
     acc_im = ai;
-    if constexpr (STATS) *s2 = sq;
+    if constexpr (STATS) {
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < G; ++i) t += sq[i];
+        *s2 = t;
+    }
 }
 
 template <int N>
@@ -372,9 +397,12 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     double* s_lo = s_mt + 2 * ntp * N;          // [2][N][bd]
     double* s_hist = s_lo + 2 * N * bd;         // mode 1
     unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
+    double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);  // [N]
     for (int i = tid; i < 2 * terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < 2 * ntp * N; i += bd) s_mt[i] = pb.mt[i];
     const int mode = pb.mode;
+    if (mode != 0)
+        for (int i = tid; i < N; i += bd) s_bnd[i] = pb.bnd[i];
     if (mode == 1)
         for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
     __syncthreads();
@@ -387,8 +415,10 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
     unsigned long long u0, u1;
     balanced_range(pb.units, T, t, &u0, &u1);
+    if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[2] = {{0.0, 0.0}, {0.0, 0.0}};
     HistCache hc;
+    int bmax = 0;
     if (u0 < u1) {
         double xr[N], xi[N];
         const unsigned long long g0 = gray_of(u0);
@@ -414,8 +444,9 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
                 double ub = 1.0;
 #pragma unroll
                 for (int r = 0; r < N; ++r)
-                    ub = mul_rn(ub, add_rn(__dsqrt_rn(__fma_rn(xr[r], xr[r], mul_rn(xi[r], xi[r]))), pb.bnd[r]));
+                    ub = mul_rn(ub, add_rn(__dsqrt_rn(__fma_rn(xr[r], xr[r], mul_rn(xi[r], xi[r]))), s_bnd[r]));
                 b = hist_bin(ub);
+                bmax = b > bmax ? b : bmax;
                 if (mode == 2 && b >= pb.thr_bin) {
                     unsigned long long k = atomicAdd(pb.list_n, 1ull);
                     if (k < pb.list_cap) {
@@ -459,6 +490,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
         }
     }
     if (mode == 1) {
+        pb.tmax[t] = (unsigned short)bmax;
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);

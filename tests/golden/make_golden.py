@@ -110,8 +110,9 @@ def make(name, threads):
     else:
         fx["hex"] = [float(v).hex() for v in a.ravel()]
         if kind == "sparse":
-            # the exact value of the matrix as given (no decomposition)
-            fx["exact"] = frac_str(O.exact_perm(a, threads=threads))
+            # exact folds (oracle/decompose.py) then exact CRT on the pieces
+            import decompose as D
+            fx["exact"] = frac_str(D.exact_perm_sparse(a))
         else:
             fx["exact"] = frac_str(O.exact_perm(a, threads=threads))
         fx["reference"] = reference_run(a, threads)
