@@ -32,8 +32,11 @@ struct Cfg {
     static constexpr int TERMS = 1 << W;
     static constexpr int NTOP = N - 1 - W;
     static constexpr int NTP = NTOP > 0 ? NTOP : 0;
-    // doubles per warp: DE table, high columns, x0 hi/lo, row exponents (as doubles)
-    static constexpr int SMEM_DOUBLES = TERMS * N * C + NTP * N * C + 2 * N * C + N;
+    // doubles per warp: DE table, high columns, x0 hi/lo, row exponents (as
+    // doubles), rounded up to 32 bytes: the unit evaluator reads the DE table
+    // with 16-byte vector loads, so every warp's slice must start aligned.
+    static constexpr int SMEM_DOUBLES = (TERMS * N * C + NTP * N * C + 2 * N * C + N + 3) / 4 * 4;
+    static_assert(SMEM_DOUBLES % 4 == 0, "per-warp shared slice must keep 32-byte alignment");
 };
 
 template <int N, int C>
