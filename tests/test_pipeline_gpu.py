@@ -107,3 +107,21 @@ def test_cli_complex(spb, tmp_path):
     assert m, out
     assert abs(float(m.group(1)) - math.factorial(12)) <= 1e-12 * math.factorial(12)
     assert abs(float(m.group(2))) <= 1e-12 * math.factorial(12)
+
+
+@pytest.mark.parametrize("args", [(), ("calculation_precision=dd",), ("algorithm=xshared_mshared",),
+                                  ("algorithm=xshared_mshared", "calculation_precision=dd")])
+def test_pipeline_sparse_n40_golden(spb, oracle, args):
+    """Config C3 (n=40: random permutation + 3 extra nonzeros per row, values
+    U[0.5,1.5)) through pruning, components, decomposition and the GPU walks,
+    against the exact value (oracle/decompose.py); the reference CPU binary's
+    sparse path is 6.4e-12 away from it."""
+    from conftest import load_golden
+    a, exact, g = load_golden("sparse_n40_s5")
+    st, out = pipeline(a, *args)
+    assert st == 0, _lib.last_error()
+    err = oracle.rel_err(out.permanent, exact)
+    print(args, "pieces", out.pieces, "avg n", out.avg_n, "rel err", err, "time", out.time_s)
+    assert err <= 1e-12
+    ref_err = oracle.rel_err(float(g["reference"]["value"]), exact)
+    assert ref_err < 1e-9
