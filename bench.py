@@ -340,18 +340,114 @@ def ours_arm(args, wl):
     return 0
 
 
+# --------------------------------------------------------- serving (C5) --
+SERVE_WORKLOADS = {
+    # name: (n_lo, n_hi, requests, description)
+    "serve": (8, 32, 20000, "serve_mixed_n8-32_real+complex_20k"),
+    "serve_small": (8, 20, 20000, "serve_mixed_n8-20_real+complex_20k"),
+}
+
+
+def make_stream(n_lo, n_hi, count, seed=2026):
+    """Seeded request stream: n uniform in [n_lo, n_hi], half real U[0,1)
+    matrices, half n x n blocks (random offsets) of Haar-random 256 x 256
+    unitaries; Poisson arrival gaps drawn separately."""
+    import numpy as np
+    from superman_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    unitaries = [W.haar_unitary(256, seed + k) for k in range(4)]
+    out = []
+    for i in range(count):
+        n = int(rng.integers(n_lo, n_hi + 1))
+        if rng.random() < 0.5:
+            out.append(W.dense_uniform(n, seed * 1000003 + i))
+        else:
+            u = unitaries[i % 4]
+            r0, c0 = rng.integers(0, 256 - n + 1, size=2)
+            out.append(np.ascontiguousarray(u[r0:r0 + n, c0:c0 + n]))
+    return out
+
+
+def serve_arm(args, wl):
+    import numpy as np
+    import superman_b200 as S
+    from superman_b200 import _lib
+    from superman_b200.serving import Server, now
+
+    n_lo, n_hi, count, desc = SERVE_WORKLOADS[wl]
+    count = args.requests or count
+    mats = make_stream(n_lo, n_hi, count)
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0 / args.rate, size=count) if args.rate > 0 else np.zeros(count)
+
+    def one_at_a_time(sample):
+        t0 = time.perf_counter()
+        for a in sample:
+            if np.iscomplexobj(a):
+                S.perm_complex(a)
+            else:
+                S.perm_dense(a)
+        return time.perf_counter() - t0
+
+    one_at_a_time(mats[:50])  # warm-up (contexts, kernel attributes)
+    with Server(max_batch=2048, slots=4, max_wait_s=args.max_wait) as srv:
+        for a in mats[:200]:  # warm-up: capture the batch shapes
+            srv.wait(srv.submit(a))
+        tickets, t_next = [], now()
+        t_first = now()
+        for a, g in zip(mats, gaps):
+            t_next += g
+            while now() < t_next:
+                pass
+            while True:
+                try:
+                    tickets.append(srv.submit(a))
+                    break
+                except S.SupermanError as e:
+                    if e.status != _lib.SPB_ERR_BUSY:
+                        raise
+                    time.sleep(50e-6)
+        res = [srv.wait(t, timeout_s=600) for t in tickets]
+        stats = srv.stats()
+    lat = np.array([r["latency_s"] for r in res])
+    span = max(r["done_s"] for r in res) - t_first
+    served = count / span
+    # one request at a time through the plain entry points, same stream
+    t_base = one_at_a_time(mats)
+    base = count / t_base
+    for a, r in list(zip(mats, res))[:64]:  # spot check against the single-call results
+        want = S.perm_complex(a).permanent if np.iscomplexobj(a) else S.perm_dense(a).permanent
+        assert abs(r["permanent"] - want) <= 1e-12 * abs(want), "served result differs from alone"
+    line = {"metric": "served_perms_per_s", "value": served, "unit": "perms/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": span * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "requests": count, "arrival_rate_per_s": args.rate or "saturating",
+                       "max_wait_s": args.max_wait},
+            "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
+                           "max": float(lat.max() * 1e3)},
+            "one_at_a_time": {"value": base, "unit": "perms/s", "seconds": t_base},
+            "speedup_vs_one_at_a_time": served / base, "server_stats": stats}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="dense32")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(SERVE_WORKLOADS), default="dense32")
+    ap.add_argument("--requests", type=int, default=0, help="serving: stream length (0 = workload default)")
+    ap.add_argument("--rate", type=float, default=0.0, help="serving: Poisson arrivals per s (0 = saturating)")
+    ap.add_argument("--max-wait", type=float, default=200e-6, help="serving: batch fill window (s)")
     ap.add_argument("--precision", choices=["fp64", "dd"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload in SERVE_WORKLOADS:
+        return serve_arm(args, args.workload)
     if args.impl == "reference":
         return reference_arm(args, args.workload)
     return ours_arm(args, args.workload)

@@ -204,6 +204,56 @@ SPB_API int spb_dm_prune(const double* a, int n, double* out, int* has_perfect_m
 SPB_API int spb_decompose(const double* a, int n, int* count, int* sizes, double* data, int max_pieces,
                           size_t max_doubles);
 
+/* ------------------------------------------------------- serving ---- */
+/* A request loop for many permanents of mixed sizes (no counterpart in the
+ * reference, which computes one matrix per process run).  Requests are
+ * admitted while the device memory they would occupy fits the budget, small
+ * ones (n <= batch_max_n) are packed per (n, real/complex) into batched
+ * launches (one warp per matrix, each batch shape captured once in a CUDA
+ * graph and replayed), large ones run the whole-GPU walk on a second stream,
+ * so both kinds overlap on the device.  A request's result does not depend on
+ * what it was batched with. */
+typedef struct spb_server_config {
+    int device;
+    int batch_max_n;      /* n <= this goes through batched launches (1..24; 0 = 20) */
+    int max_batch;        /* matrices per batched launch (0 = 2048)                 */
+    int slots;            /* batched launches in flight (0 = 4)                     */
+    double max_wait_s;    /* longest a small request waits for its batch to fill   */
+    size_t admit_bytes;   /* admission budget: queued matrices' bytes (0 = 256 MiB) */
+    int precision;        /* enum spb_precision for large requests                  */
+    int use_graphs;       /* >= 0: replay captured batch shapes (default); < 0: plain launches */
+} spb_server_config;
+
+typedef struct spb_request_result {
+    double re, re_lo, im, im_lo; /* the permanent (double-double per component) */
+    double submit_s, done_s;     /* steady-clock seconds: admission, completion */
+    int n, is_complex;
+    int status;                  /* SPB_OK, SPB_ERR_CANCELLED or a failure       */
+} spb_request_result;
+
+typedef struct spb_server_stats {
+    uint64_t submitted, completed, rejected, cancelled;
+    uint64_t batches, batched_requests, graph_launches, graphs_captured, large_launches;
+    size_t queued_bytes;
+} spb_server_stats;
+
+SPB_API int spb_server_create(const spb_server_config* cfg, void** server);
+/* Copies the row-major matrix (interleaved re/im when is_complex); SPB_ERR_BUSY
+ * when admission refuses it. */
+SPB_API int spb_server_submit(void* server, const double* a, int n, int is_complex, uint64_t* ticket);
+/* SPB_OK and the result when done (the ticket is then released), SPB_ERR_BUSY
+ * while pending, SPB_ERR_INVALID for an unknown ticket. */
+SPB_API int spb_server_poll(void* server, uint64_t ticket, spb_request_result* out);
+/* Like poll but waits up to timeout_s; SPB_ERR_TIMEOUT if still pending. */
+SPB_API int spb_server_wait(void* server, uint64_t ticket, double timeout_s, spb_request_result* out);
+/* Cancels a queued request (SPB_OK); an in-flight one completes as cancelled. */
+SPB_API int spb_server_cancel(void* server, uint64_t ticket);
+SPB_API int spb_server_get_stats(void* server, spb_server_stats* out);
+/* Stops the workers after the work in flight and frees the server. */
+SPB_API int spb_server_destroy(void* server);
+/* Steady-clock seconds on the clock the request timestamps use. */
+SPB_API double spb_now(void);
+
 /* Measured pipe throughput used as the roofline denominator: which = 0 gives
  * FP64 FMA thread-instructions per second, which = 1 gives int32 multiply-add
  * thread-instructions per second (best of three timed launches).  No

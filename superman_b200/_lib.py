@@ -82,6 +82,34 @@ class spb_pipeline_result(ctypes.Structure):
     ]
 
 
+class spb_server_config(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int),
+        ("batch_max_n", ctypes.c_int),
+        ("max_batch", ctypes.c_int),
+        ("slots", ctypes.c_int),
+        ("max_wait_s", ctypes.c_double),
+        ("admit_bytes", ctypes.c_size_t),
+        ("precision", ctypes.c_int),
+        ("use_graphs", ctypes.c_int),
+    ]
+
+
+class spb_request_result(ctypes.Structure):
+    _fields_ = [
+        ("re", ctypes.c_double), ("re_lo", ctypes.c_double),
+        ("im", ctypes.c_double), ("im_lo", ctypes.c_double),
+        ("submit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+        ("n", ctypes.c_int), ("is_complex", ctypes.c_int), ("status", ctypes.c_int),
+    ]
+
+
+class spb_server_stats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in (
+        "submitted", "completed", "rejected", "cancelled", "batches", "batched_requests",
+        "graph_launches", "graphs_captured", "large_launches")] + [("queued_bytes", ctypes.c_size_t)]
+
+
 _DP = ctypes.POINTER(ctypes.c_double)
 _OP = ctypes.POINTER(spb_options)
 _RP = ctypes.POINTER(spb_result)
@@ -112,6 +140,16 @@ SIGNATURES = {
     "spb_dm_prune": (ctypes.c_int, [_DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int)]),
     "spb_decompose": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), _DP, ctypes.c_int, ctypes.c_size_t]),
+    "spb_server_create": (ctypes.c_int, [ctypes.POINTER(spb_server_config), ctypes.POINTER(ctypes.c_void_p)]),
+    "spb_server_submit": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "spb_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(spb_request_result)]),
+    "spb_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                       ctypes.POINTER(spb_request_result)]),
+    "spb_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "spb_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(spb_server_stats)]),
+    "spb_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "spb_now": (ctypes.c_double, []),
     "spb_measure_pipe_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_double)]),
 }
