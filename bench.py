@@ -42,6 +42,10 @@ WORKLOADS = {
     "dense24": ("dense", 24, 3, "dense_f64_u01_n24_seed3"),
     "dense28": ("dense", 28, 28, "dense_f64_u01_n28_seed28"),
     "complex28": ("complex", 28, 6, "complex128_haar256_block_n28_seed6"),
+    "binary36": ("binary", 36, 4, "binary_bernoulli0.5_or_identity_n36_seed4"),
+    "binary28": ("binary", 28, 4, "binary_bernoulli0.5_or_identity_n28_seed4"),
+    "batch20": ("batch", 20, 11, "batch_4096_dense_u01_n20_seed11"),
+    "sparse40": ("sparse", 40, 5, "sparse_perm_plus3_u0.5-1.5_n40_seed5"),
 }
 
 # DRAM bytes per walk launch from one ncu capture of this workload
@@ -395,18 +399,29 @@ def serve_arm(args, wl):
             srv.wait(srv.submit(a))
         tickets, t_next = [], now()
         t_first = now()
-        for a, g in zip(mats, gaps):
-            t_next += g
-            while now() < t_next:
-                pass
-            while True:
-                try:
-                    tickets.append(srv.submit(a))
-                    break
-                except S.SupermanError as e:
-                    if e.status != _lib.SPB_ERR_BUSY:
-                        raise
+        if args.rate <= 0:
+            # saturating arrivals: bulk submission, refused requests retried
+            pending = list(mats)
+            while pending:
+                got = srv.submit_many(pending[:1024])
+                tickets += [t for t in got if t]
+                refused = [a for a, t in zip(pending[:1024], got) if not t]
+                pending = refused + pending[1024:]
+                if refused:
                     time.sleep(50e-6)
+        else:
+            for a, g in zip(mats, gaps):
+                t_next += g
+                while now() < t_next:
+                    pass
+                while True:
+                    try:
+                        tickets.append(srv.submit(a))
+                        break
+                    except S.SupermanError as e:
+                        if e.status != _lib.SPB_ERR_BUSY:
+                            raise
+                        time.sleep(50e-6)
         res = [srv.wait(t, timeout_s=600) for t in tickets]
         stats = srv.stats()
     lat = np.array([r["latency_s"] for r in res])
@@ -431,6 +446,120 @@ def serve_arm(args, wl):
     return 0
 
 
+def other_arm(args, wl):
+    """0/1 exact and sparse-pipeline workloads (one GPU, device-event timing)."""
+    import numpy as np
+    import superman_b200 as S
+    from superman_b200 import _lib, workloads as W
+    kind, n, seed, desc = WORKLOADS[wl]
+    L = _lib.lib()
+    peak = ctypes.c_double()
+    if kind == "batch":
+        import torch
+        count = 4096
+        mats = np.stack([W.dense_uniform(n, seed * 100000 + k) for k in range(count)])
+        d_in = torch.from_numpy(mats).cuda()
+        d_out = torch.empty(count * 2, dtype=torch.float64, device="cuda")
+        _lib.check(L.spb_measure_pipe_peak(0, 0, ctypes.byref(peak)))
+
+        def step():
+            _lib.check(L.spb_perm_batch_dev(ctypes.c_void_p(d_in.data_ptr()), n, 0, count,
+                                            ctypes.c_void_p(d_out.data_ptr()), None))
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                step()
+            torch.cuda.synchronize()  # device-wide: the launches run on the library's default stream
+            t = (time.perf_counter() - t0) / args.steps
+        alg = count * 2 * n * 2 ** (n - 1)
+        got = d_out.cpu().numpy()[0::2]
+        want0 = S.perm_dense(mats[0]).permanent
+        assert abs(got[0] - want0) <= 1e-13 * abs(want0)
+        line = {"metric": "batched_perms_per_s", "value": count / t, "unit": "perms/s",
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "n": n, "count": count,
+                           "gray_steps_per_s": count * n * 2 ** (n - 1) / t,
+                           "timing": "host clock around the launches, device-wide synchronize after"},
+                "roofline": {"bound": "fp64", "achieved": alg / t / 1e12, "peak": peak.value / 1e12,
+                             "unit": "T FP64-pipe inst/s", "frac": alg / t / peak.value, "traffic": None},
+                "clocks": clk.summary(), "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+        return 0
+    if kind == "binary":
+        a = W.binary_bernoulli(n, seed)
+        _lib.check(L.spb_measure_pipe_peak(0, 1, ctypes.byref(peak)))
+        for _ in range(args.warmup):
+            r = S.perm_binary(a)
+        with ClockSampler(0) as clk:
+            rs = [S.perm_binary(a) for _ in range(args.steps)]
+        assert all(x.permanent == rs[0].permanent for x in rs)
+        t = statistics.mean(x.kernel_s for x in rs)
+        dt = statistics.mean(x.time for x in rs)
+        steps = n * 2 ** n
+        alg = 2 * steps  # one integer add + one multiply per row per subset
+        line = {"metric": "ryser_gray_steps_per_s", "value": steps / t, "unit": "gray-steps/s (plain Ryser, n*2^n)",
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/u128",
+                "data": "synthetic",
+                "config": {"workload": desc, "n": n, "seed": seed, "permanent": str(rs[0].permanent),
+                           "nw_equivalent_gray_steps_per_s": n * 2 ** (n - 1) / t},
+                "roofline": {"bound": "int", "achieved": alg / t / 1e12, "peak": peak.value / 1e12,
+                             "unit": "T int32 ops/s (add+mul per row-update) vs IMAD pipe",
+                             "frac": alg / t / peak.value, "traffic": None},
+                "clocks": clk.summary(), "gpu_launches": args.steps}
+    else:
+        a = W.sparse_perm_plus(n, seed)
+        arr = (ctypes.c_char_p * 1)(b"calculation_precision=" + args.precision.replace("fp64", "kahan").encode())
+        out = _lib.spb_pipeline_result()
+        def step():
+            t0 = time.perf_counter()
+            _lib.check(L.spb_perm_pipeline(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n, arr, 1,
+                                           ctypes.byref(out)))
+            return time.perf_counter() - t0
+        for _ in range(args.warmup):
+            step()
+        with ClockSampler(0) as clk:
+            ts = [step() for _ in range(args.steps)]
+        t = statistics.mean(ts)
+        err = None
+        gpath = os.path.join(ROOT, "tests", "golden", "sparse_n40_s5.json")
+        if os.path.exists(gpath) and n == 40 and seed == 5:
+            from fractions import Fraction
+            ex = Fraction(json.load(open(gpath))["exact"])
+            err = float(abs(Fraction(out.permanent) - ex) / ex)
+        line = {"metric": "sparse_pipeline_perms_per_s", "value": 1.0 / t, "unit": "perms/s",
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "n": n, "seed": seed, "pieces": out.pieces, "avg_piece_n": out.avg_n,
+                           "components": out.components, "permanent": repr(out.permanent),
+                           "rel_err_vs_exact": err, "precision": args.precision,
+                           "timing": "host wall clock around spb_perm_pipeline (pruning, decomposition, GPU pieces)"},
+                "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "m.mtx")
+            write_mtx(p, a.astype(np.float64))
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            if os.path.exists(O.ref_binary_path()):
+                v, secs = O.run_reference(p, threads=cores, timeout=1800)
+                line["cpu_baseline"] = {"value": (1.0 / secs) if kind == "sparse" else (n * 2 ** (n - 1) / secs),
+                                        "unit": line["unit"] if kind == "sparse" else "gray-steps/s (NW)",
+                                        "cores": cores, "kind": "reference",
+                                        "sample": f"reference CPU binary on the same matrix, {secs:.3f} s",
+                                        "permanent": v}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -441,7 +570,9 @@ def main():
     ap.add_argument("--requests", type=int, default=0, help="serving: stream length (0 = workload default)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: Poisson arrivals per s (0 = saturating)")
     ap.add_argument("--max-wait", type=float, default=200e-6, help="serving: batch fill window (s)")
-    ap.add_argument("--precision", choices=["fp64", "dd"], default="fp64")
+    # dd: the accuracy bar of the headline (<= 1e-12 relative at n=32) needs the
+    # double-double re-evaluation of the dominant units; fp64 is ~3e-12 there.
+    ap.add_argument("--precision", choices=["fp64", "dd"], default="dd")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -450,6 +581,8 @@ def main():
         return serve_arm(args, args.workload)
     if args.impl == "reference":
         return reference_arm(args, args.workload)
+    if WORKLOADS[args.workload][0] in ("binary", "sparse", "batch"):
+        return other_arm(args, args.workload)
     return ours_arm(args, args.workload)
 
 

@@ -241,6 +241,12 @@ SPB_API int spb_server_create(const spb_server_config* cfg, void** server);
 /* Copies the row-major matrix (interleaved re/im when is_complex); SPB_ERR_BUSY
  * when admission refuses it. */
 SPB_API int spb_server_submit(void* server, const double* a, int n, int is_complex, uint64_t* ticket);
+/* Submits `count` matrices in one call (sizes ns[k], flags is_complex[k],
+ * entries concatenated row-major in `mats`); tickets[k] receives each ticket,
+ * or 0 where admission refused the matrix.  Returns the number admitted in
+ * *admitted.  For clients that receive requests in bulk. */
+SPB_API int spb_server_submit_many(void* server, const double* mats, const int* ns, const int* is_complex,
+                                   int count, uint64_t* tickets, int* admitted);
 /* SPB_OK and the result when done (the ticket is then released), SPB_ERR_BUSY
  * while pending, SPB_ERR_INVALID for an unknown ticket. */
 SPB_API int spb_server_poll(void* server, uint64_t ticket, spb_request_result* out);

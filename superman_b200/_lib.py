@@ -143,6 +143,9 @@ SIGNATURES = {
     "spb_server_create": (ctypes.c_int, [ctypes.POINTER(spb_server_config), ctypes.POINTER(ctypes.c_void_p)]),
     "spb_server_submit": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "spb_server_submit_many": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]),
     "spb_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(spb_request_result)]),
     "spb_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
                                        ctypes.POINTER(spb_request_result)]),

@@ -544,6 +544,28 @@ extern "C" int spb_server_submit(void* server, const double* a, int n, int is_co
     return static_cast<Server*>(server)->submit(a, n, is_complex ? 2 : 1, ticket);
 }
 
+extern "C" int spb_server_submit_many(void* server, const double* mats, const int* ns, const int* is_complex,
+                                      int count, uint64_t* tickets, int* admitted)
+{
+    if (!server || !mats || !ns || !tickets || count < 0) return SPB_ERR_INVALID;
+    auto* s = static_cast<Server*>(server);
+    size_t off = 0;
+    int ok = 0;
+    for (int k = 0; k < count; ++k) {
+        const int c = (is_complex && is_complex[k]) ? 2 : 1;
+        tickets[k] = 0;
+        const int st = s->submit(mats + off, ns[k], c, &tickets[k]);
+        if (st == SPB_OK) ++ok;
+        else if (st != SPB_ERR_BUSY) {
+            if (admitted) *admitted = ok;
+            return st;
+        }
+        off += (size_t)ns[k] * ns[k] * c;
+    }
+    if (admitted) *admitted = ok;
+    return SPB_OK;
+}
+
 extern "C" int spb_server_poll(void* server, uint64_t ticket, spb_request_result* out)
 {
     if (!server) return SPB_ERR_INVALID;

@@ -33,6 +33,27 @@ class Server:
                                                 a.shape[0], int(is_c), ctypes.byref(t)))
         return t.value
 
+    def submit_many(self, mats):
+        """Queues a list of matrices in one C call; returns their tickets (0
+        where admission refused one)."""
+        flat, ns, cx = [], [], []
+        for a in mats:
+            a = np.asarray(a)
+            c = np.iscomplexobj(a)
+            b = np.ascontiguousarray(a, dtype=np.complex128 if c else np.float64)
+            flat.append((b.view(np.float64) if c else b).ravel())
+            ns.append(a.shape[0])
+            cx.append(int(c))
+        buf = np.concatenate(flat) if flat else np.zeros(1)
+        k = len(ns)
+        n_arr = (ctypes.c_int * max(1, k))(*ns)
+        c_arr = (ctypes.c_int * max(1, k))(*cx)
+        t_arr = (ctypes.c_uint64 * max(1, k))()
+        got = ctypes.c_int()
+        _lib.check(_lib.lib().spb_server_submit_many(self._h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                     n_arr, c_arr, k, t_arr, ctypes.byref(got)))
+        return [t_arr[i] for i in range(k)]
+
     def poll(self, ticket):
         """The request's result dict when done, else None."""
         r = _lib.spb_request_result()
