@@ -178,9 +178,19 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     size_t o_hs = take(sizeof(double) * kHistBins);
     size_t o_hc = take(sizeof(unsigned long long) * kHistBins);
     size_t o_ln = take(sizeof(unsigned long long) * 2);
-    size_t o_tm = pb->mode != 0 ? take(sizeof(unsigned short) * (size_t)pb->grid * pb->threads) : 0;
+    const size_t T = (size_t)pb->grid * pb->threads;
+    const bool refine = pb->mode != 0;
+    size_t o_tm = refine ? take(sizeof(unsigned short) * T) : 0;
+    size_t o_co = refine ? take(sizeof(unsigned) * T * kCand) : 0;
+    size_t o_cb = refine ? take(sizeof(unsigned short) * T * kCand) : 0;
+    size_t o_cn = refine ? take(T) : 0;
+    size_t o_cd = refine ? take(sizeof(int) * 4) : 0;
     if (base) {
-        pb->tmax = pb->mode != 0 ? reinterpret_cast<unsigned short*>(base + o_tm) : nullptr;
+        pb->tmax = refine ? reinterpret_cast<unsigned short*>(base + o_tm) : nullptr;
+        pb->cand_off = refine ? reinterpret_cast<unsigned*>(base + o_co) : nullptr;
+        pb->cand_bin = refine ? reinterpret_cast<unsigned short*>(base + o_cb) : nullptr;
+        pb->cand_n = refine ? reinterpret_cast<unsigned char*>(base + o_cn) : nullptr;
+        pb->cand_dropped = refine ? reinterpret_cast<int*>(base + o_cd) : nullptr;
         pb->bnd = reinterpret_cast<double*>(base + o_bnd);
         pb->hist_s2 = reinterpret_cast<double*>(base + o_hs);
         pb->hist_cnt = reinterpret_cast<unsigned long long*>(base + o_hc);
@@ -310,6 +320,7 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
     if (dd_mode) {
         SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_s2, 0, sizeof(double) * kHistBins, stream));
         SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_cnt, 0, sizeof(unsigned long long) * kHistBins, stream));
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.cand_dropped, 0xff, sizeof(int), stream));  // -1
     }
     setup_kernel<<<1, 512, 0, stream>>>(pb, d_a);
     SPB_CUDA_TRY(cudaGetLastError());
@@ -330,9 +341,14 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
         // First pass done: read its total and the unit histogram.
         static thread_local double hs2[kHistBins];
         static thread_local unsigned long long hcnt[kHistBins];
+        int dropped = -1;
         SPB_CUDA_TRY(cudaMemcpyAsync(hs2, pb.hist_s2, sizeof(hs2), cudaMemcpyDeviceToHost, stream));
         SPB_CUDA_TRY(cudaMemcpyAsync(hcnt, pb.hist_cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaMemcpyAsync(&dropped, pb.cand_dropped, sizeof(int), cudaMemcpyDeviceToHost, stream));
         SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+        int gmax = 0;
+        for (int b = 0; b < kHistBins; ++b)
+            if (hcnt[b]) gmax = b;
         const double tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
         const double mag = comps == 1 ? std::fabs(h.res[0].hi) : std::hypot(h.res[0].hi, h.res[1].hi);
         unsigned long long count = 0;
@@ -343,20 +359,36 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
             const size_t entry = sizeof(double) * 2 * n * comps;
             if ((st = ensure_list(ctx, count * (entry + sizeof(unsigned long long)) + 256)) != SPB_OK)
                 return out->status = st;
-            pb.mode = 2;
             pb.thr_bin = thr;
             pb.list_cap = count;
             pb.list_u = static_cast<unsigned long long*>(ctx->list);
-            pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
-                                                  align_up(count * sizeof(unsigned long long), 256));
-            SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+            unsigned long long listed = 0;
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
-            if ((st = launch_walk(pb, blocks, threads, smem, stream)) != SPB_OK) return out->status = st;
+            // Fast path: every unit at or above the threshold sits in the
+            // per-thread candidate lists when the threshold is within the
+            // candidate span of the highest bin and no list dropped such a unit.
+            bool fast = thr >= gmax - kCandSpan && dropped < thr;
+            if (fast) {
+                pb.list_x = nullptr;
+                SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+                if ((st = launch_collect(pb, blocks, threads, stream)) != SPB_OK) return out->status = st;
+                SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
+                SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+                fast = listed == count;
+                launches += 1;
+            }
+            if (!fast) {  // scan: replay the walk and list the units with their bases
+                pb.mode = 2;
+                pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
+                                                      align_up(count * sizeof(unsigned long long), 256));
+                SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+                if ((st = launch_walk(pb, blocks, threads, smem, stream)) != SPB_OK) return out->status = st;
+                launches += 1;
+            }
             if ((st = launch_refine(pb, count, blocks, stream)) != SPB_OK) return out->status = st;
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref1, stream));
-            launches += 2;
+            launches += 1;
             dd corr[2];
-            unsigned long long listed = 0;
             SPB_CUDA_TRY(cudaMemcpyAsync(corr, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
             SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
             SPB_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -365,6 +397,7 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
                               (unsigned long long)listed, (unsigned long long)count);
                 return out->status = SPB_ERR_CUDA;
             }
+            out->refined_units = count;
             for (int cc = 0; cc < comps; ++cc) h.res[cc] = dd_add(h.res[cc], corr[cc]);
             float mr = 0.f;
             SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));

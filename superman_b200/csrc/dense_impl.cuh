@@ -37,6 +37,50 @@ struct Problem {
     unsigned long long* list_u;    // [list_cap] unit index
     double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
     unsigned short* tmax;          // [grid*threads] highest bound bin of each thread's units
+    // mode 1 candidate lists: units within kCandSpan bins of the thread's running
+    // maximum, up to kCand per thread (offset from the thread's first unit, bin)
+    unsigned* cand_off;            // [grid*threads][kCand]
+    unsigned short* cand_bin;      // [grid*threads][kCand]
+    unsigned char* cand_n;         // [grid*threads]
+    int* cand_dropped;             // highest bin evicted from any full list (atomicMax)
+};
+
+constexpr int kCand = 8;
+constexpr int kCandSpan = 8;  // bins (4 octaves each)
+
+// Per-thread candidate list kept in global memory (insertions are rare: only
+// units near the thread's running maximum bound).
+struct CandList {
+    int rmax = -1, count = 0, minbin = 1 << 30, minidx = 0, dropped = -1;
+    __device__ __forceinline__ void add(const Problem& pb, unsigned long long t, unsigned off, int b)
+    {
+        if (b > rmax) rmax = b;
+        if (b < rmax - kCandSpan) return;
+        unsigned* co = pb.cand_off + t * kCand;
+        unsigned short* cb = pb.cand_bin + t * kCand;
+        if (count < kCand) {
+            co[count] = off;
+            cb[count] = (unsigned short)b;
+            if (b < minbin) { minbin = b; minidx = count; }
+            ++count;
+            return;
+        }
+        if (b <= minbin) {
+            dropped = b > dropped ? b : dropped;
+            return;
+        }
+        dropped = minbin > dropped ? minbin : dropped;
+        co[minidx] = off;
+        cb[minidx] = (unsigned short)b;
+        minbin = 1 << 30;
+        for (int k = 0; k < kCand; ++k)
+            if ((int)cb[k] < minbin) { minbin = cb[k]; minidx = k; }
+    }
+    __device__ __forceinline__ void close(const Problem& pb, unsigned long long t)
+    {
+        pb.cand_n[t] = (unsigned char)count;
+        if (dropped >= 0) atomicMax(pb.cand_dropped, dropped);
+    }
 };
 
 // Unit-bound histogram: bin = (ilogb(U) + 1024) / 4, i.e. four octaves per bin.
@@ -252,6 +296,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[1] = {{0.0, 0.0}};
     HistCache hc;
+    CandList cl;
     int bmax = 0;
     if (u0 < u1) {
         double xh[N];
@@ -294,6 +339,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
                 double us = unit_sum_real<N, G, true>(xh, s_de, nq, &sq);
                 tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
                 hc.add(b, sq, s_hist, s_cnt);  // actual sum of squared terms, keyed by the bound
+                cl.add(pb, t, (unsigned)(u - u0), b);
             }
             if (++u >= u1) break;
             const int j = __ffsll((long long)u) - 1;
@@ -311,6 +357,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     }
     if (mode == 1) {
         pb.tmax[t] = (unsigned short)bmax;
+        cl.close(pb, t);
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
@@ -418,6 +465,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[2] = {{0.0, 0.0}, {0.0, 0.0}};
     HistCache hc;
+    CandList cl;
     int bmax = 0;
     if (u0 < u1) {
         double xr[N], xi[N];
@@ -469,7 +517,10 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
                 if (u & 1ull) { ur = -ur; ui = -ui; }
                 tot[0] = dd_add_d(tot[0], ur);
                 tot[1] = dd_add_d(tot[1], ui);
-                if (mode == 1) hc.add(b, sq, s_hist, s_cnt);
+                if (mode == 1) {
+                    hc.add(b, sq, s_hist, s_cnt);
+                    cl.add(pb, t, (unsigned)(u - u0), b);
+                }
             }
             if (++u >= u1) break;
             const int j = __ffsll((long long)u) - 1;
@@ -491,6 +542,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     }
     if (mode == 1) {
         pb.tmax[t] = (unsigned short)bmax;
+        cl.close(pb, t);
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
@@ -502,6 +554,11 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
 // accumulates (double-double unit sum - the walk's FP64 unit sum) into
 // pb.result, one warp per unit.  Defined in dense_refine.cu.
 int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s);
+
+// Fast path: turns the mode-1 candidate lists into the list of units whose
+// bin >= pb.thr_bin (pb.list_u, count in *pb.list_n); the refine kernel then
+// rebuilds each unit base from scratch (pb.list_x == nullptr).
+int launch_collect(const Problem& pb, int blocks, int threads, cudaStream_t s);
 
 // Per-n dispatch (defined in the instantiation units).
 int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);

@@ -78,6 +78,39 @@ __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const dou
     }
 }
 
+// Unit base of unit u (component `part`) rebuilt from scratch in
+// double-double the way the walk builds a thread's first unit (x0 plus the
+// selected high columns in index order); lanes take rows.
+__device__ __forceinline__ void unit_base(const Problem& pb, unsigned long long u, int part, int lane, double* hi,
+                                          double* lo)
+{
+    const int n = pb.n, ntop = n - 1 - pb.w;
+    const unsigned long long g = gray_of(u);
+    const double* mt = pb.mt + (size_t)part * (ntop > 0 ? ntop : 0) * n;
+    for (int r = lane; r < n; r += 32) {
+        dd x = {pb.x0_hi[part * n + r], pb.x0_lo[part * n + r]};
+        for (int j = 0; j < ntop; ++j)
+            if ((g >> j) & 1ull) x = dd_add_d(x, mt[j * n + r]);
+        hi[r] = x.hi;
+        lo[r] = x.lo;
+    }
+}
+
+__global__ void collect_candidates(Problem pb)
+{
+    const unsigned long long T = (unsigned long long)pb.grid * pb.threads;
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    unsigned long long u0, u1;
+    balanced_range(pb.units, T, t, &u0, &u1);
+    const int cnt = pb.cand_n[t];
+    for (int k = 0; k < cnt; ++k)
+        if ((int)pb.cand_bin[t * kCand + k] >= pb.thr_bin) {
+            const unsigned long long i = atomicAdd(pb.list_n, 1ull);
+            if (i < pb.list_cap) pb.list_u[i] = u0 + pb.cand_off[t * kCand + k];
+        }
+}
+
 __global__ void __launch_bounds__(256) refine_real(Problem pb, unsigned long long count)
 {
     extern __shared__ __align__(16) double sm[];
@@ -97,8 +130,12 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb, unsigned long lon
     dd corr = {0.0, 0.0};
     for (unsigned long long e = (unsigned long long)blockIdx.x * nwarps + wid; e < count;
          e += (unsigned long long)gridDim.x * nwarps) {
-        const double* src = pb.list_x + e * (2 * n);
-        for (int i = lane; i < 2 * n; i += 32) xw[i] = src[i];
+        if (pb.list_x) {
+            const double* src = pb.list_x + e * (2 * n);
+            for (int i = lane; i < 2 * n; i += 32) xw[i] = src[i];
+        } else {
+            unit_base(pb, pb.list_u[e], 0, lane, xw, xw + n);
+        }
         __syncwarp();
         for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, G);
         dd acc = {0.0, 0.0};
@@ -150,8 +187,13 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
     dd corr_r = {0.0, 0.0}, corr_i = {0.0, 0.0};
     for (unsigned long long e = (unsigned long long)blockIdx.x * nwarps + wid; e < count;
          e += (unsigned long long)gridDim.x * nwarps) {
-        const double* src = pb.list_x + e * (4 * n);
-        for (int i = lane; i < 4 * n; i += 32) xw[i] = src[i];
+        if (pb.list_x) {
+            const double* src = pb.list_x + e * (4 * n);
+            for (int i = lane; i < 4 * n; i += 32) xw[i] = src[i];
+        } else {
+            unit_base(pb, pb.list_u[e], 0, lane, xw, xw + n);
+            unit_base(pb, pb.list_u[e], 1, lane, xw + 2 * n, xw + 3 * n);
+        }
         __syncwarp();
         for (int q = lane; q < nq; q += 32)
             group_sum_complex_rt(xw, xw + 2 * n, drh + q * n * G, dih + q * n * G, n, G, gw[2 * q],
@@ -208,6 +250,14 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
 }
 
 }  // namespace
+
+int launch_collect(const Problem& pb, int blocks, int threads, cudaStream_t s)
+{
+    const unsigned long long T = (unsigned long long)blocks * threads;
+    collect_candidates<<<(unsigned)((T + 255) / 256), 256, 0, s>>>(pb);
+    SPB_CUDA_TRY(cudaGetLastError());
+    return SPB_OK;
+}
 
 size_t refine_smem_bytes(const Problem& pb, int threads)
 {
