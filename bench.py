@@ -537,7 +537,8 @@ def other_arm(args, wl):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": desc, "n": n, "seed": seed, "pieces": out.pieces, "avg_piece_n": out.avg_n,
-                           "components": out.components, "permanent": repr(out.permanent),
+                           "components": out.components, "algorithm": out.algorithm,
+                           "permanent": repr(out.permanent),
                            "rel_err_vs_exact": err, "precision": args.precision,
                            "timing": "host wall clock around spb_perm_pipeline (pruning, decomposition, GPU pieces)"},
                 "clocks": clk.summary()}

@@ -9,7 +9,8 @@
 //    re-evaluation of dominant terms, KAHAN the FP64 walk.
 //  * spbSparseSingleGPU<C,S> the sparse driver: orders the columns by
 //    ascending degree and builds the CSR/CSC view as the reference's sparse
-//    drivers do (CommonFiles/Permanent.h:82-87), then walks the pattern.
+//    drivers do (CommonFiles/Permanent.h:82-87), then hands the CSC arrays to
+//    spb_perm_sparse_f64 (row-compacted walk when its cost model wins).
 //  * binary=true on a 0/1 matrix computes the exact integer permanent.
 #pragma once
 
@@ -73,6 +74,21 @@ inline double dense_permanent(const Matrix<S>* m, const Settings& s)
     return r.value + r.value_lo;
 }
 
+// The sparse driver's permanent: the compressed-column arrays of the
+// SparseMatrix go to spb_perm_sparse_f64 (row-compacted walk when it pays).
+template <class S>
+inline double sparse_permanent(const SparseMatrix<S>* m, const Settings& s)
+{
+    const int n = m->nov;
+    if (n == 0) return 1.0;
+    if (s.binary && is01(m)) return dense_permanent(m, s);
+    spb_options o = options_from(s);
+    spb_result r;
+    std::vector<double> vals(m->cvals, m->cvals + m->cptrs[n]);
+    check(spb_perm_sparse_f64(m->cptrs, m->rows, vals.data(), n, &o, &r));
+    return r.value + r.value_lo;
+}
+
 }  // namespace spb_detail
 
 template <class C, class S>
@@ -86,7 +102,12 @@ template <class C, class S>
 class spbSparseSingleGPU : public Permanent<C, S> {
 public:
     spbSparseSingleGPU(Matrix<S>* matrix, Settings settings) : Permanent<C, S>(matrix, settings) {}
-    double permanentFunction() final { return spb_detail::dense_permanent(this->m_Matrix, this->m_Settings); }
+    double permanentFunction() final
+    {
+        if (auto* sp = dynamic_cast<SparseMatrix<S>*>(this->m_Matrix))
+            return spb_detail::sparse_permanent(sp, this->m_Settings);
+        return spb_detail::dense_permanent(this->m_Matrix, this->m_Settings);
+    }
 
 protected:
     void prepare() override

@@ -50,6 +50,13 @@ enum spb_precision {
     SPB_PREC_DD = 1    /* + double-double re-evaluation of dominant units    */
 };
 
+/* Walk used by spb_perm_sparse_f64. */
+enum spb_sparse_walk {
+    SPB_SPARSE_WALK_AUTO = 0,   /* row-compacted walk when its cost model wins   */
+    SPB_SPARSE_WALK_NEVER = 1,  /* always the dense walk                         */
+    SPB_SPARSE_WALK_ALWAYS = 2  /* row-compacted walk whenever the pattern allows */
+};
+
 typedef struct spb_options {
     int device;            /* CUDA ordinal (Settings::deviceID)              */
     int precision;         /* enum spb_precision                             */
@@ -58,6 +65,7 @@ typedef struct spb_options {
     int threads_per_block; /* 0 = automatic                                  */
     int blocks;            /* 0 = automatic (persistent: one CTA per SM)     */
     void* stream;          /* cudaStream_t to run on; NULL = library stream  */
+    int sparse_walk;       /* enum spb_sparse_walk (spb_perm_sparse_f64)     */
 } spb_options;
 
 typedef struct spb_result {
@@ -74,6 +82,8 @@ typedef struct spb_result {
     uint64_t refined_units;/* units re-evaluated in double-double           */
     int status;            /* enum spb_status                               */
     int launches;          /* kernels launched by the call                  */
+    int active_rows;       /* rows varying inside a Gray unit: n for the
+                              dense walk, fewer for the row-compacted walk  */
 } spb_result;
 
 /* Fills *opt with the defaults (device 0, SPB_PREC_FP64, automatic shape). */
@@ -96,8 +106,30 @@ SPB_API int spb_device_count(void);
  * dpSingleGPU<C,S,Algo,Shared>::permanentFunction
  * (Algorithms/GPU/Dense/dpSingleGPU.cuh:45-219) and its kernels
  * xRegisterMShared[Kahan] (Algorithms/GPU/Dense/DenseKernelDefinitions.cuh:
- * 189-264, 331-405).  a: n*n doubles, row-major. */
+ * 189-264, 331-405).  a: n*n doubles, row-major.  A matrix with zeros may
+ * run on the row-compacted walk of spb_perm_sparse_f64 when its cost model
+ * wins (opt->sparse_walk; out->active_rows < n then). */
 SPB_API int spb_perm_dense_f64(const double* a, int n, const spb_options* opt, spb_result* out);
+
+/* Sparse real permanent from compressed-column arrays, the layout of the
+ * reference's SparseMatrix (Structures/SparseMatrix.h:61-101): column c holds
+ * rows[cptrs[c] .. cptrs[c+1]-1] with values cvals[...]; nnz = cptrs[n];
+ * duplicate entries are summed.  Replaces spSingleGPU<C,S,Algo>::
+ * permanentFunction (Algorithms/GPU/Sparse/spSingleGPU.cuh:45-234) with its
+ * kernels (Algorithms/GPU/Sparse/SparseKernelDefinitions.cuh:33-509), and the
+ * per-matrix generated kernels (Algorithms/GPU/CodeGeneration/
+ * KernelGenerator.cuh:114-176): rows and columns are permuted so that the
+ * rows varying inside a Gray unit are few, and a walk compiled for that row
+ * count runs (opt->sparse_walk; out->active_rows reports it). */
+SPB_API int spb_perm_sparse_f64(const int* cptrs, const int* rows, const double* cvals, int n,
+                                const spb_options* opt, spb_result* out);
+
+/* The plan spb_perm_sparse_f64 would run for a row-major n x n matrix under
+ * sparse_walk `mode`, without running it: *na active rows (n = the dense
+ * walk), *w low columns, and the row and column orders (new position ->
+ * original index; either may be NULL).  In the permuted matrix rows
+ * na..n-1 are zero in columns 0..w-1.  CPU only. */
+SPB_API int spb_sparse_plan(const double* a, int n, int mode, int* na, int* w, int* row_order, int* col_order);
 
 /* Same on a device-resident row-major matrix. */
 SPB_API int spb_perm_dense_f64_dev(const double* d_a, int n, const spb_options* opt,

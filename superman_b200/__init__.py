@@ -17,10 +17,11 @@ import numpy as np
 from . import _lib
 from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
 
-__all__ = ["Result", "perm_dense", "perm_complex", "perm_binary", "SupermanError", "SPB_PREC_FP64",
-           "SPB_PREC_DD", "device_count"]
+__all__ = ["Result", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "SupermanError",
+           "SPB_PREC_FP64", "SPB_PREC_DD", "device_count"]
 
 _PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD}
+_SPARSE_WALK = {"auto": 0, "never": 1, "always": 2}
 
 
 @dataclass
@@ -36,6 +37,7 @@ class Result:
     gray_steps: int = 0
     refined_units: int = 0
     launches: int = 0
+    active_rows: int = 0
 
 
 def device_count() -> int:
@@ -51,7 +53,7 @@ def _to_result(r: _lib.spb_result, complex_: bool) -> Result:
     val = complex(r.value, r.imag) if complex_ else r.value
     return Result(time=r.elapsed_s, permanent=val, permanent_lo=r.value_lo, imag_lo=r.imag_lo,
                   kernel_s=r.kernel_s, err_est=r.err_est, gray_steps=r.gray_steps,
-                  refined_units=r.refined_units, launches=r.launches)
+                  refined_units=r.refined_units, launches=r.launches, active_rows=r.active_rows)
 
 
 def perm_dense(a, precision="fp64", device: int = 0, **shape) -> Result:
@@ -63,6 +65,40 @@ def perm_dense(a, precision="fp64", device: int = 0, **shape) -> Result:
     opt = _options(precision, device, **shape)
     st = _lib.lib().spb_perm_dense_f64(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                        a.shape[0], ctypes.byref(opt), ctypes.byref(out))
+    _lib.check(st)
+    return _to_result(out, False)
+
+
+def perm_sparse(a, precision="fp64", device: int = 0, walk: str = "auto", **shape) -> Result:
+    """Permanent of a sparse real n x n matrix (1 <= n <= 63), given dense or
+    as a (cptrs, rows, cvals) compressed-column triple like the reference's
+    SparseMatrix.  walk: "auto" (cost model), "never" (dense walk) or
+    "always" (row-compacted walk whenever the pattern allows);
+    Result.active_rows tells which ran."""
+    if isinstance(a, tuple):
+        cptrs, rows, cvals = a
+        cptrs = np.ascontiguousarray(cptrs, dtype=np.int32)
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        cvals = np.ascontiguousarray(cvals, dtype=np.float64)
+        n = cptrs.size - 1
+    else:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise ValueError("perm_sparse needs a square 2-D array or a (cptrs, rows, cvals) triple")
+        n = a.shape[0]
+        r_idx, c_idx = np.nonzero(a.T)  # column-major order: (column, row) pairs
+        cptrs = np.zeros(n + 1, dtype=np.int32)
+        np.add.at(cptrs, r_idx + 1, 1)
+        cptrs = np.cumsum(cptrs).astype(np.int32)
+        rows = np.ascontiguousarray(c_idx, dtype=np.int32)
+        cvals = np.ascontiguousarray(a.T[r_idx, c_idx], dtype=np.float64)
+    out = _lib.spb_result()
+    opt = _options(precision, device, **shape)
+    opt.sparse_walk = _SPARSE_WALK[walk]
+    ip = ctypes.POINTER(ctypes.c_int)
+    st = _lib.lib().spb_perm_sparse_f64(cptrs.ctypes.data_as(ip), rows.ctypes.data_as(ip),
+                                        cvals.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n,
+                                        ctypes.byref(opt), ctypes.byref(out))
     _lib.check(st)
     return _to_result(out, False)
 

@@ -48,6 +48,7 @@ class spb_options(ctypes.Structure):
         ("threads_per_block", ctypes.c_int),
         ("blocks", ctypes.c_int),
         ("stream", ctypes.c_void_p),
+        ("sparse_walk", ctypes.c_int),
     ]
 
 
@@ -65,6 +66,7 @@ class spb_result(ctypes.Structure):
         ("refined_units", ctypes.c_uint64),
         ("status", ctypes.c_int),
         ("launches", ctypes.c_int),
+        ("active_rows", ctypes.c_int),
     ]
 
 
@@ -122,6 +124,11 @@ SIGNATURES = {
     "spb_version": (ctypes.c_int, []),
     "spb_device_count": (ctypes.c_int, []),
     "spb_perm_dense_f64": (ctypes.c_int, [_DP, ctypes.c_int, _OP, _RP]),
+    "spb_sparse_plan": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "spb_perm_sparse_f64": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _DP,
+                                           ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_f64_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128": (ctypes.c_int, [_DP, ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_c128_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),

@@ -85,12 +85,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
             s_de[part * TERMS * N + ((d / G) * N + r) * G + (d % G)] = s.hi;
         }
         // high columns [part][j][r]
-        for (int idx = lane; idx < NTP * N * C; idx += 32) {
-            const int part = idx / (NTP * N), rem = idx % (NTP * N);
-            const int j = rem / N, r = rem % N;
-            s_mt[idx] = ldexp(A[(r * N + (W + j)) * C + part], -s_exp[r]);
-            (void)part;
-        }
+        if constexpr (NTP > 0)
+            for (int idx = lane; idx < NTP * N * C; idx += 32) {
+                const int part = idx / (NTP * N), rem = idx % (NTP * N);
+                const int j = rem / N, r = rem % N;
+                s_mt[idx] = ldexp(A[(r * N + (W + j)) * C + part], -s_exp[r]);
+            }
         __syncwarp();
 
         unsigned long long u0, u1;

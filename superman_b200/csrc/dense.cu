@@ -29,7 +29,9 @@
 #include <cstring>
 
 #include "context.h"
+#include "dense_host.h"
 #include "dense_impl.cuh"
+#include "sparse_impl.cuh"
 #include "spb_common.cuh"
 
 namespace spb {
@@ -181,16 +183,19 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     const size_t T = (size_t)pb->grid * pb->threads;
     const bool refine = pb->mode != 0;
     size_t o_tm = refine ? take(sizeof(unsigned short) * T) : 0;
-    size_t o_co = refine ? take(sizeof(unsigned) * T * kCand) : 0;
-    size_t o_cb = refine ? take(sizeof(unsigned short) * T * kCand) : 0;
-    size_t o_cn = refine ? take(T) : 0;
-    size_t o_cd = refine ? take(sizeof(int) * 4) : 0;
+    size_t o_pc = refine ? take(sizeof(unsigned) * kHistBins) : 0;
+    size_t o_lb = refine ? take(sizeof(int) * 4) : 0;
+    size_t o_rn = refine ? take(sizeof(unsigned long long) * 2) : 0;
+    size_t o_ru = refine ? take(sizeof(unsigned long long) * kRawCap) : 0;
+    size_t o_rb = refine ? take(sizeof(unsigned short) * kRawCap) : 0;
     if (base) {
         pb->tmax = refine ? reinterpret_cast<unsigned short*>(base + o_tm) : nullptr;
-        pb->cand_off = refine ? reinterpret_cast<unsigned*>(base + o_co) : nullptr;
-        pb->cand_bin = refine ? reinterpret_cast<unsigned short*>(base + o_cb) : nullptr;
-        pb->cand_n = refine ? reinterpret_cast<unsigned char*>(base + o_cn) : nullptr;
-        pb->cand_dropped = refine ? reinterpret_cast<int*>(base + o_cd) : nullptr;
+        pb->pre_cnt = refine ? reinterpret_cast<unsigned*>(base + o_pc) : nullptr;
+        pb->list_bin = refine ? reinterpret_cast<int*>(base + o_lb) : nullptr;
+        pb->raw_n = refine ? reinterpret_cast<unsigned long long*>(base + o_rn) : nullptr;
+        pb->raw_cap = refine ? kRawCap : 0;
+        pb->raw_u = refine ? reinterpret_cast<unsigned long long*>(base + o_ru) : nullptr;
+        pb->raw_b = refine ? reinterpret_cast<unsigned short*>(base + o_rb) : nullptr;
         pb->bnd = reinterpret_cast<double*>(base + o_bnd);
         pb->hist_s2 = reinterpret_cast<double*>(base + o_hs);
         pb->hist_cnt = reinterpret_cast<unsigned long long*>(base + o_hc);
@@ -213,6 +218,7 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
 size_t walk_smem_bytes(const Problem& pb, int threads)
 {
     const int n = pb.n, c = pb.comps;
+    if (pb.na < n) return sparse_smem_bytes(n, pb.na, pb.w, threads);
     size_t terms = (size_t)1 << pb.w;
     int ntop = n - 1 - pb.w;
     return sizeof(double) * (terms * n * c + (size_t)(ntop > 0 ? ntop : 0) * n * c +
@@ -249,8 +255,8 @@ static int pick_threshold(const double* s2, const unsigned long long* cnt, int n
     return b;
 }
 
-static int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in,
-               spb_result* out)
+int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in, spb_result* out,
+        const WalkPlan* plan)
 {
     double t_start = wall_seconds();
     if (!out) {
@@ -273,13 +279,22 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
 
     Problem pb{};
     pb.n = n;
+    pb.na = n;
     pb.comps = comps;
     pb.w = choose_unit_bits(n, comps, &opt);
+    if (plan && plan->na < n) {
+        if (comps != 1 || plan->na < 1 || plan->na > kMaxActive || plan->w < 2 || plan->w > n - 2) {
+            spb_set_error("row-compacted walk: bad plan (n=%d, active rows %d, w=%d)", n, plan->na, plan->w);
+            return out->status = SPB_ERR_INVALID;
+        }
+        pb.na = plan->na;
+        pb.w = plan->w;
+    }
     pb.g = group_size(n, comps);
     pb.units = 1ull << (n - 1 - pb.w);
 
     int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 0;
-    const int max_threads = walk_max_threads(n, comps);
+    const int max_threads = pb.na < n ? 512 : walk_max_threads(n, comps);
     if (threads == 0) {
         threads = max_threads;
         // fit the per-thread lo vectors next to the tables
@@ -320,15 +335,26 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
     if (dd_mode) {
         SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_s2, 0, sizeof(double) * kHistBins, stream));
         SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_cnt, 0, sizeof(unsigned long long) * kHistBins, stream));
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.cand_dropped, 0xff, sizeof(int), stream));  // -1
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.pre_cnt, 0, sizeof(unsigned) * kHistBins, stream));
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.raw_n, 0, sizeof(unsigned long long), stream));
     }
     setup_kernel<<<1, 512, 0, stream>>>(pb, d_a);
     SPB_CUDA_TRY(cudaGetLastError());
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
+    int launches = 2;
+    if (dd_mode && pb.na == n) {
+        // Size the first pass's unit list from a bound-only pass (about 1.5 %
+        // of a dense walk).  The row-compacted walk has few terms per unit, so
+        // there the pass would cost a large share; it lists nothing and a
+        // refinement, when one is needed, goes through the scan.
+        if ((st = launch_bound_pass(pb, blocks, stream)) != SPB_OK) return out->status = st;
+        launches += 2;
+    } else if (dd_mode) {  // 0x7f7f7f7f: above every bin
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.list_bin, 0x7f, sizeof(int), stream));
+    }
     st = launch_walk(pb, blocks, threads, smem, stream);
     if (st != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
-    int launches = 2;
 
     struct {
         dd res[2];
@@ -341,14 +367,13 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
         // First pass done: read its total and the unit histogram.
         static thread_local double hs2[kHistBins];
         static thread_local unsigned long long hcnt[kHistBins];
-        int dropped = -1;
+        int list_bin = kHistBins;
+        unsigned long long raw_n = 0;
         SPB_CUDA_TRY(cudaMemcpyAsync(hs2, pb.hist_s2, sizeof(hs2), cudaMemcpyDeviceToHost, stream));
         SPB_CUDA_TRY(cudaMemcpyAsync(hcnt, pb.hist_cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, stream));
-        SPB_CUDA_TRY(cudaMemcpyAsync(&dropped, pb.cand_dropped, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaMemcpyAsync(&list_bin, pb.list_bin, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaMemcpyAsync(&raw_n, pb.raw_n, sizeof(raw_n), cudaMemcpyDeviceToHost, stream));
         SPB_CUDA_TRY(cudaStreamSynchronize(stream));
-        int gmax = 0;
-        for (int b = 0; b < kHistBins; ++b)
-            if (hcnt[b]) gmax = b;
         const double tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
         const double mag = comps == 1 ? std::fabs(h.res[0].hi) : std::hypot(h.res[0].hi, h.res[1].hi);
         unsigned long long count = 0;
@@ -364,14 +389,14 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
             pb.list_u = static_cast<unsigned long long*>(ctx->list);
             unsigned long long listed = 0;
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
-            // Fast path: every unit at or above the threshold sits in the
-            // per-thread candidate lists when the threshold is within the
-            // candidate span of the highest bin and no list dropped such a unit.
-            bool fast = thr >= gmax - kCandSpan && dropped < thr;
+            // Fast path: the first pass listed every unit at or above list_bin;
+            // when the threshold is not below it and the list did not
+            // overflow, the units to refine are all in that list.
+            bool fast = thr >= list_bin && raw_n <= pb.raw_cap;
             if (fast) {
                 pb.list_x = nullptr;
                 SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
-                if ((st = launch_collect(pb, blocks, threads, stream)) != SPB_OK) return out->status = st;
+                if ((st = launch_collect(pb, stream)) != SPB_OK) return out->status = st;
                 SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
                 SPB_CUDA_TRY(cudaStreamSynchronize(stream));
                 fast = listed == count;
@@ -424,6 +449,7 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
     out->device_s = ms_call * 1e-3;
     out->gray_steps = (uint64_t)n << (n - 1);
     out->launches = launches;
+    out->active_rows = pb.na;
     out->status = SPB_OK;
     out->elapsed_s = wall_seconds() - t_start;
     return SPB_OK;
@@ -432,24 +458,26 @@ static int run(const double* a, bool a_on_device, int n, int comps, const spb_op
 }  // namespace dense
 }  // namespace spb
 
-extern "C" int spb_perm_dense_f64(const double* a, int n, const spb_options* opt, spb_result* out)
+extern "C" int spb_perm_dense_f64(const double* a, int n, const spb_options* opt_in, spb_result* out)
 {
-    return spb::dense::run(a, false, n, 1, opt, out);
+    spb_options opt;
+    if (opt_in) opt = *opt_in; else spb_default_options(&opt);
+    return spb::dense::run_real_host(a, n, &opt, out);
 }
 
 extern "C" int spb_perm_dense_f64_dev(const double* d_a, int n, const spb_options* opt,
                                       spb_result* out)
 {
-    return spb::dense::run(d_a, true, n, 1, opt, out);
+    return spb::dense::run(d_a, true, n, 1, opt, out, nullptr);
 }
 
 extern "C" int spb_perm_dense_c128(const double* a, int n, const spb_options* opt, spb_result* out)
 {
-    return spb::dense::run(a, false, n, 2, opt, out);
+    return spb::dense::run(a, false, n, 2, opt, out, nullptr);
 }
 
 extern "C" int spb_perm_dense_c128_dev(const double* d_a, int n, const spb_options* opt,
                                        spb_result* out)
 {
-    return spb::dense::run(d_a, true, n, 2, opt, out);
+    return spb::dense::run(d_a, true, n, 2, opt, out, nullptr);
 }

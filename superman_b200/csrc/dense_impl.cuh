@@ -15,6 +15,8 @@ constexpr int kMaxN = 63;
 // scratch arena written by setup_kernel.
 struct Problem {
     int n, comps, w, g, grid, threads;
+    int na;                    // rows that vary within a unit: n (dense walk) or the
+                               // active rows of the row-compacted walk (sparse_impl.cuh)
     unsigned long long units;  // 2^(n-1-w) Gray units of 2^w terms each
     double* as;                // row-scaled matrix (row-major, comps interleaved)
     double* x0_hi;             // [comps][n] NW start vector, double-double
@@ -37,51 +39,31 @@ struct Problem {
     unsigned long long* list_u;    // [list_cap] unit index
     double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
     unsigned short* tmax;          // [grid*threads] highest bound bin of each thread's units
-    // mode 1 candidate lists: units within kCandSpan bins of the thread's running
-    // maximum, up to kCand per thread (offset from the thread's first unit, bin)
-    unsigned* cand_off;            // [grid*threads][kCand]
-    unsigned short* cand_bin;      // [grid*threads][kCand]
-    unsigned char* cand_n;         // [grid*threads]
-    int* cand_dropped;             // highest bin evicted from any full list (atomicMax)
+    // Mode 1 direct listing: bound_pass counts the units per bound bin
+    // (pre_cnt), pick_list_bin sets *list_bin to the lowest bin whose tail fits
+    // raw_cap, and the walk appends every unit at or above it (raw_*).
+    unsigned* pre_cnt;             // [kHistBins]
+    int* list_bin;
+    unsigned long long* raw_n;
+    unsigned long long raw_cap;
+    unsigned long long* raw_u;     // [raw_cap] unit index
+    unsigned short* raw_b;         // [raw_cap] its bound bin
 };
 
-constexpr int kCand = 8;
-constexpr int kCandSpan = 8;  // bins (4 octaves each)
+// Capacity of the mode-1 list (units); pick_list_bin aims at half of it so
+// that bins computed by the walk and by bound_pass may differ at bin edges.
+constexpr unsigned long long kRawCap = 1ull << 17;
 
-// Per-thread candidate list kept in global memory (insertions are rare: only
-// units near the thread's running maximum bound).
-struct CandList {
-    int rmax = -1, count = 0, minbin = 1 << 30, minidx = 0, dropped = -1;
-    __device__ __forceinline__ void add(const Problem& pb, unsigned long long t, unsigned off, int b)
-    {
-        if (b > rmax) rmax = b;
-        if (b < rmax - kCandSpan) return;
-        unsigned* co = pb.cand_off + t * kCand;
-        unsigned short* cb = pb.cand_bin + t * kCand;
-        if (count < kCand) {
-            co[count] = off;
-            cb[count] = (unsigned short)b;
-            if (b < minbin) { minbin = b; minidx = count; }
-            ++count;
-            return;
-        }
-        if (b <= minbin) {
-            dropped = b > dropped ? b : dropped;
-            return;
-        }
-        dropped = minbin > dropped ? minbin : dropped;
-        co[minidx] = off;
-        cb[minidx] = (unsigned short)b;
-        minbin = 1 << 30;
-        for (int k = 0; k < kCand; ++k)
-            if ((int)cb[k] < minbin) { minbin = cb[k]; minidx = k; }
+// Appends unit u (bound bin b) to the mode-1 list when b >= lbin.
+__device__ __forceinline__ void raw_list_add(const Problem& pb, int lbin, unsigned long long u, int b)
+{
+    if (b < lbin) return;
+    const unsigned long long k = atomicAdd(pb.raw_n, 1ull);
+    if (k < pb.raw_cap) {
+        pb.raw_u[k] = u;
+        pb.raw_b[k] = (unsigned short)b;
     }
-    __device__ __forceinline__ void close(const Problem& pb, unsigned long long t)
-    {
-        pb.cand_n[t] = (unsigned char)count;
-        if (dropped >= 0) atomicMax(pb.cand_dropped, dropped);
-    }
-};
+}
 
 // Unit-bound histogram: bin = (ilogb(U) + 1024) / 4, i.e. four octaves per bin.
 constexpr int kHistBins = 512;
@@ -296,7 +278,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[1] = {{0.0, 0.0}};
     HistCache hc;
-    CandList cl;
+    const int lbin = mode == 1 ? __ldcg(pb.list_bin) : 0;
     int bmax = 0;
     if (u0 < u1) {
         double xh[N];
@@ -339,7 +321,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
                 double us = unit_sum_real<N, G, true>(xh, s_de, nq, &sq);
                 tot[0] = dd_add_d(tot[0], (u & 1ull) ? -us : us);
                 hc.add(b, sq, s_hist, s_cnt);  // actual sum of squared terms, keyed by the bound
-                cl.add(pb, t, (unsigned)(u - u0), b);
+                raw_list_add(pb, lbin, u, b);
             }
             if (++u >= u1) break;
             const int j = __ffsll((long long)u) - 1;
@@ -357,7 +339,6 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     }
     if (mode == 1) {
         pb.tmax[t] = (unsigned short)bmax;
-        cl.close(pb, t);
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
@@ -465,7 +446,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     if (mode == 2 && (int)pb.tmax[t] < pb.thr_bin) u1 = u0;
     dd tot[2] = {{0.0, 0.0}, {0.0, 0.0}};
     HistCache hc;
-    CandList cl;
+    const int lbin = mode == 1 ? __ldcg(pb.list_bin) : 0;
     int bmax = 0;
     if (u0 < u1) {
         double xr[N], xi[N];
@@ -519,7 +500,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
                 tot[1] = dd_add_d(tot[1], ui);
                 if (mode == 1) {
                     hc.add(b, sq, s_hist, s_cnt);
-                    cl.add(pb, t, (unsigned)(u - u0), b);
+                    raw_list_add(pb, lbin, u, b);
                 }
             }
             if (++u >= u1) break;
@@ -542,7 +523,6 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     }
     if (mode == 1) {
         pb.tmax[t] = (unsigned short)bmax;
-        cl.close(pb, t);
         hc.flush(s_hist, s_cnt);
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
@@ -555,17 +535,23 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
 // pb.result, one warp per unit.  Defined in dense_refine.cu.
 int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s);
 
-// Fast path: turns the mode-1 candidate lists into the list of units whose
-// bin >= pb.thr_bin (pb.list_u, count in *pb.list_n); the refine kernel then
+// Mode-1 listing support (dense_refine.cu): bound_pass + pick_list_bin run
+// before the walk; collect then keeps the listed units whose bin >=
+// pb.thr_bin (pb.list_u, count in *pb.list_n), and the refine kernel
 // rebuilds each unit base from scratch (pb.list_x == nullptr).
-int launch_collect(const Problem& pb, int blocks, int threads, cudaStream_t s);
+int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s);
+int launch_collect(const Problem& pb, cudaStream_t s);
 
 // Per-n dispatch (defined in the instantiation units).
 int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
 int launch_walk_complex(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
 
+// Row-compacted walk on NA = pb.na active rows (sparse_walk.cu).
+int launch_walk_sparse(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+
 inline int launch_walk(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s)
 {
+    if (pb.na < pb.n) return launch_walk_sparse(pb, blocks, threads, smem, s);
     return pb.comps == 1 ? launch_walk_real(pb, blocks, threads, smem, s)
                          : launch_walk_complex(pb, blocks, threads, smem, s);
 }

@@ -6,9 +6,11 @@
 // final error.  The walk (mode 1) bins every unit by an upper bound U_u of its
 // terms and accumulates the unit's actual sum of squared terms in that bin;
 // the host picks the bin from which the remaining units' rounding error fits
-// the tolerance; a scan (walk mode 2, same launch shape, so the unit bases
-// are bit-identical) lists the units at or above it with their double-double
-// base vectors; this kernel then re-evaluates each listed unit, one warp per
+// the tolerance.  The units at or above it come from the walk's own list
+// (every unit at or above a bin chosen beforehand by bound_walk, when that
+// bin is low enough), or else from a scan (walk mode 2, same launch shape, so
+// the unit bases are bit-identical) that lists them with their double-double
+// base vectors.  This kernel then re-evaluates each listed unit, one warp per
 // unit:
 //   * the FP64 unit sum exactly as the walk computed it (same operations in
 //     the same order, so the same bits), spread over the lanes by group;
@@ -17,14 +19,17 @@
 // and accumulates sign_u * (dd_sum - fp64_sum) into pb.result.  Adding that
 // correction to the walk's total replaces the dominant units' FP64 values by
 // their double-double values.
+#include "bound_impl.cuh"
 #include "dense_impl.cuh"
 
 namespace spb {
 namespace dense {
 namespace {
 
-// One group of G terms, bitwise identical to unit_sum_real<N,G>'s group.
-__device__ __forceinline__ double group_sum_real_rt(const double* xh, const double* de, int n, int G)
+// One group of G terms, bitwise identical to unit_sum_real<N,G>'s group
+// (na == n) or to unit_sum_sparse<NA>'s (na < n: the inactive rows' product
+// first, then the na active rows; see sparse_impl.cuh).
+__device__ __forceinline__ double group_sum_real_rt(const double* xh, const double* de, int n, int na, int G)
 {
     double p0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
     p0 = add_rn(xh[0], de[0]);
@@ -33,7 +38,15 @@ __device__ __forceinline__ double group_sum_real_rt(const double* xh, const doub
         p2 = add_rn(xh[0], de[2]);
         p3 = add_rn(xh[0], de[3]);
     }
-    for (int r = 1; r < n; ++r) {
+    if (na < n) {
+        double c = xh[na];
+        for (int r = na + 1; r < n; ++r) c = mul_rn(c, xh[r]);
+        p0 = mul_rn(c, p0);
+        p1 = mul_rn(c, p1);
+        p2 = mul_rn(c, p2);
+        p3 = mul_rn(c, p3);
+    }
+    for (int r = 1; r < na; ++r) {
         const double x = xh[r];
         p0 = mul_rn(p0, add_rn(x, de[r * G + 0]));
         if (G >= 2) p1 = mul_rn(p1, add_rn(x, de[r * G + 1]));
@@ -96,18 +109,30 @@ __device__ __forceinline__ void unit_base(const Problem& pb, unsigned long long 
     }
 }
 
-__global__ void collect_candidates(Problem pb)
+// *list_bin = the lowest bin whose tail (units at or above it) holds
+// at most raw_cap/2 units by bound_walk's count.
+__global__ void pick_list_bin(Problem pb)
 {
-    const unsigned long long T = (unsigned long long)pb.grid * pb.threads;
-    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= T) return;
-    unsigned long long u0, u1;
-    balanced_range(pb.units, T, t, &u0, &u1);
-    const int cnt = pb.cand_n[t];
-    for (int k = 0; k < cnt; ++k)
-        if ((int)pb.cand_bin[t * kCand + k] >= pb.thr_bin) {
+    __shared__ unsigned s_c[kHistBins];
+    for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) s_c[i] = pb.pre_cnt[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long tail = 0;
+        int b = kHistBins;
+        while (b > 0 && tail + s_c[b - 1] <= pb.raw_cap / 2) tail += s_c[--b];
+        *pb.list_bin = b;
+    }
+}
+
+// Keeps the mode-1 listed units whose bin >= thr_bin.
+__global__ void collect_listed(Problem pb)
+{
+    const unsigned long long m = *pb.raw_n < pb.raw_cap ? *pb.raw_n : pb.raw_cap;
+    for (unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; e < m;
+         e += (unsigned long long)gridDim.x * blockDim.x)
+        if ((int)pb.raw_b[e] >= pb.thr_bin) {
             const unsigned long long i = atomicAdd(pb.list_n, 1ull);
-            if (i < pb.list_cap) pb.list_u[i] = u0 + pb.cand_off[t * kCand + k];
+            if (i < pb.list_cap) pb.list_u[i] = pb.raw_u[e];
         }
 }
 
@@ -137,7 +162,7 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb, unsigned long lon
             unit_base(pb, pb.list_u[e], 0, lane, xw, xw + n);
         }
         __syncwarp();
-        for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, G);
+        for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, pb.na, G);
         dd acc = {0.0, 0.0};
         for (int d = lane; d < terms; d += 32) {
             const int q = d / G, i = d % G;
@@ -251,10 +276,36 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
 
 }  // namespace
 
-int launch_collect(const Problem& pb, int blocks, int threads, cudaStream_t s)
+template <int N>
+int launch_bound_n(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+
+int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s)
 {
-    const unsigned long long T = (unsigned long long)blocks * threads;
-    collect_candidates<<<(unsigned)((T + 255) / 256), 256, 0, s>>>(pb);
+    const int threads = 256;
+    const size_t smem = bound_smem_bytes_f(pb.n, pb.comps, pb.w);
+    blocks *= 2;  // two CTAs per SM
+    unsigned long long max_blocks = (pb.units + threads - 1) / threads;
+    if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
+    if (blocks < 1) blocks = 1;
+    int st = SPB_ERR_INVALID;
+    switch (pb.n) {
+#define SPB_CASE(N) \
+    case N: st = launch_bound_n<N>(pb, blocks, threads, smem, s); break;
+        SPB_FOR_EACH_N(SPB_CASE)
+#undef SPB_CASE
+    default:
+        spb_set_error("bound pass: n=%d outside 1..%d", pb.n, kMaxN);
+        return SPB_ERR_INVALID;
+    }
+    if (st != SPB_OK) return st;
+    pick_list_bin<<<1, 128, 0, s>>>(pb);
+    SPB_CUDA_TRY(cudaGetLastError());
+    return SPB_OK;
+}
+
+int launch_collect(const Problem& pb, cudaStream_t s)
+{
+    collect_listed<<<(unsigned)((pb.raw_cap + 255) / 256), 256, 0, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }

@@ -108,6 +108,7 @@ extern "C" int spb_perm_dense_f64_noalloc(const double* d_a, int n, double* d_ou
     spb_default_options(&opt);
     Problem pb{};
     pb.n = n;
+    pb.na = n;
     pb.comps = 1;
     pb.w = choose_unit_bits(n, 1, &opt);
     pb.g = group_size(n, 1);
