@@ -66,6 +66,10 @@ typedef struct spb_options {
     int blocks;            /* 0 = automatic (persistent: one CTA per SM)     */
     void* stream;          /* cudaStream_t to run on; NULL = library stream  */
     int sparse_walk;       /* enum spb_sparse_walk (spb_perm_sparse_f64)     */
+    int replay_listing;    /* SPB_PREC_DD: 1 = list the units to refine by
+                              replaying the walk (its own unit bases) instead
+                              of the first pass's list or the parallel scan;
+                              same result, slower (for verification)        */
 } spb_options;
 
 typedef struct spb_result {

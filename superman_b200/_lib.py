@@ -49,6 +49,7 @@ class spb_options(ctypes.Structure):
         ("blocks", ctypes.c_int),
         ("stream", ctypes.c_void_p),
         ("sparse_walk", ctypes.c_int),
+        ("replay_listing", ctypes.c_int),
     ]
 
 

@@ -392,17 +392,22 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
             // Fast path: the first pass listed every unit at or above list_bin;
             // when the threshold is not below it and the list did not
             // overflow, the units to refine are all in that list.
-            bool fast = thr >= list_bin && raw_n <= pb.raw_cap;
-            if (fast) {
+            // Otherwise a parallel scan lists them (bases rebuilt from scratch).
+            // Both are checked against the histogram's count; the replay scan
+            // below, whose bases are the walk's own, is the last resort.
+            const bool from_list = thr >= list_bin && raw_n <= pb.raw_cap;
+            bool fast = false;
+            if (!opt.replay_listing) {
                 pb.list_x = nullptr;
                 SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
-                if ((st = launch_collect(pb, stream)) != SPB_OK) return out->status = st;
+                st = from_list ? launch_collect(pb, stream) : launch_scan_parallel(pb, stream);
+                if (st != SPB_OK) return out->status = st;
                 SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
                 SPB_CUDA_TRY(cudaStreamSynchronize(stream));
                 fast = listed == count;
                 launches += 1;
             }
-            if (!fast) {  // scan: replay the walk and list the units with their bases
+            if (!fast) {  // replay the walk and list the units with their bases
                 pb.mode = 2;
                 pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
                                                       align_up(count * sizeof(unsigned long long), 256));

@@ -260,7 +260,9 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     double* s_lo = s_mt + (ntop > 0 ? ntop : 0) * N;
     double* s_hist = s_lo + N * bd;  // mode 1
     unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
-    double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);  // [2][N]
+    // DE range per row, [2][N] (min, max).  Two scalar loads per row: a paired
+    // 16-byte load keeps more registers live and makes the n=32 walk spill.
+    double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);
     for (int i = tid; i < terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < ntop * N; i += bd) s_mt[i] = pb.mt[i];
     const int mode = pb.mode;
@@ -541,6 +543,9 @@ int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaS
 // rebuilds each unit base from scratch (pb.list_x == nullptr).
 int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s);
 int launch_collect(const Problem& pb, cudaStream_t s);
+// Lists the units whose bin >= pb.thr_bin from the walk's per-thread maxima
+// (pb.tmax), one warp per thread range, bases rebuilt from scratch.
+int launch_scan_parallel(const Problem& pb, cudaStream_t s);
 
 // Per-n dispatch (defined in the instantiation units).
 int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);

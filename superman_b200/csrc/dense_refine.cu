@@ -8,10 +8,11 @@
 // the host picks the bin from which the remaining units' rounding error fits
 // the tolerance.  The units at or above it come from the walk's own list
 // (every unit at or above a bin chosen beforehand by bound_walk, when that
-// bin is low enough), or else from a scan (walk mode 2, same launch shape, so
-// the unit bases are bit-identical) that lists them with their double-double
-// base vectors.  This kernel then re-evaluates each listed unit, one warp per
-// unit:
+// bin is low enough), else from a parallel scan (scan_parallel), and only if
+// either count disagrees with the histogram from a replay scan (walk mode 2,
+// same launch shape, so the unit bases are bit-identical) that lists them
+// with their double-double base vectors.  This kernel then re-evaluates each
+// listed unit, one warp per unit:
 //   * the FP64 unit sum exactly as the walk computed it (same operations in
 //     the same order, so the same bits), spread over the lanes by group;
 //   * the double-double unit sum (x_r = xtop_r + DE[d][r] in double-double,
@@ -106,6 +107,90 @@ __device__ __forceinline__ void unit_base(const Problem& pb, unsigned long long 
             if ((g >> j) & 1ull) x = dd_add_d(x, mt[j * n + r]);
         hi[r] = x.hi;
         lo[r] = x.lo;
+    }
+}
+
+// The walk's unit bound (dense_impl.cuh walk_real/walk_complex, and
+// sparse_impl.cuh walk_sparse when pb.na < pb.n) from the hi words of a unit
+// base (xh: [comps][n]): the same operations in the same order.
+__device__ double unit_bound_rt(const Problem& pb, const double* xh)
+{
+    const int n = pb.n, na = pb.na;
+    double ub = 1.0;
+    if (pb.comps == 2) {
+        for (int r = 0; r < n; ++r) {
+            const double xr = xh[r], xi = xh[kMaxN + r];
+            ub = mul_rn(ub, add_rn(__dsqrt_rn(__fma_rn(xr, xr, mul_rn(xi, xi))), pb.bnd[r]));
+        }
+        return ub;
+    }
+    if (na < n) {
+        double c = xh[na];
+        for (int r = na + 1; r < n; ++r) c = mul_rn(c, xh[r]);
+        ub = fabs(c);
+    }
+    for (int r = 0; r < na; ++r)
+        ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], pb.bnd[r])), fabs(add_rn(xh[r], pb.bnd[n + r]))));
+    return ub;
+}
+
+// Parallel listing of the units whose bin >= thr_bin.  The walk's threads
+// whose highest bin reaches it (tmax) are visited one per warp; each lane
+// takes a contiguous part of that thread's units, builds the first unit base
+// from scratch in double-double and steps through the Gray order with the
+// walk's own base update, evaluating the walk's bound per unit.  Lists unit
+// indices only (the refine kernel rebuilds the bases).  A lane's bases start
+// from a rebuild rather than from the walk's thread start, so a hi word could
+// in principle differ from the walk's (a row value within ~2^-100 of a
+// rounding midpoint); if that ever moved a unit across the threshold the
+// count check fails and the caller falls back to the replay scan.
+__global__ void __launch_bounds__(128) scan_parallel(Problem pb)
+{
+    const unsigned long long T = (unsigned long long)pb.grid * pb.threads;
+    const int lane = threadIdx.x & 31, n = pb.n, c = pb.comps;
+    const int ntop = n - 1 - pb.w, ntp = ntop > 0 ? ntop : 0;
+    const unsigned long long warp = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    double xh[2 * kMaxN], xl[2 * kMaxN];  // [comps][kMaxN], per lane
+    for (unsigned long long t = warp; t < T; t += nwarps) {
+        if ((int)pb.tmax[t] < pb.thr_bin) continue;  // warp-uniform
+        unsigned long long u0, u1;
+        balanced_range(pb.units, T, t, &u0, &u1);
+        unsigned long long a, b;
+        balanced_range(u1 - u0, 32, lane, &a, &b);
+        a += u0;
+        b += u0;
+        if (a >= b) continue;
+        const unsigned long long g0 = gray_of(a);
+        for (int part = 0; part < c; ++part) {
+            const double* mt = pb.mt + (size_t)part * ntp * n;
+            for (int r = 0; r < n; ++r) {
+                dd x = {pb.x0_hi[part * n + r], pb.x0_lo[part * n + r]};
+                for (int j = 0; j < ntop; ++j)
+                    if ((g0 >> j) & 1ull) x = dd_add_d(x, mt[j * n + r]);
+                xh[part * kMaxN + r] = x.hi;
+                xl[part * kMaxN + r] = x.lo;
+            }
+        }
+        for (unsigned long long u = a;;) {
+            if (hist_bin(unit_bound_rt(pb, xh)) >= pb.thr_bin) {
+                const unsigned long long i = atomicAdd(pb.list_n, 1ull);
+                if (i < pb.list_cap) pb.list_u[i] = u;
+            }
+            if (++u >= b) break;
+            const int j = __ffsll((long long)u) - 1;
+            const bool add = (gray_of(u) >> j) & 1ull;
+            for (int part = 0; part < c; ++part) {
+                const double* col = pb.mt + ((size_t)part * ntp + j) * n;
+                for (int r = 0; r < n; ++r) {
+                    const double m = add ? col[r] : -col[r];
+                    dd s = two_sum(xh[part * kMaxN + r], m);
+                    dd z = fast_two_sum(s.hi, add_rn(s.lo, xl[part * kMaxN + r]));
+                    xh[part * kMaxN + r] = z.hi;
+                    xl[part * kMaxN + r] = z.lo;
+                }
+            }
+        }
     }
 }
 
@@ -299,6 +384,13 @@ int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s)
     }
     if (st != SPB_OK) return st;
     pick_list_bin<<<1, 128, 0, s>>>(pb);
+    SPB_CUDA_TRY(cudaGetLastError());
+    return SPB_OK;
+}
+
+int launch_scan_parallel(const Problem& pb, cudaStream_t s)
+{
+    scan_parallel<<<pb.grid * 4, 128, 0, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }

@@ -58,11 +58,15 @@ int popc(unsigned long long x) { return __builtin_popcountll(x); }
 // 2^w terms.  Per term: the x additions and products of the varying rows plus
 // the group combine; per unit: the double-double base update of the varying
 // rows, the product of the constant rows, the inactive nonzeros of the
-// flipped column (expected count `flip`), and bookkeeping.
-double walk_cost(int n, int w, int na, double flip)
+// flipped column (expected count `flip`), and bookkeeping.  The double-double
+// mode's first pass adds a squared-term accumulation per term and the unit
+// bound with its histogram update per unit.
+double walk_cost(int n, int w, int na, double flip, bool dd)
 {
     const double units = std::ldexp(1.0, n - 1 - w), terms = std::ldexp(1.0, w);
-    return units * (terms * (2.0 * na + 0.75) + 12.0 * na + 2.0 * (n - na) + 14.0 * flip + 40.0);
+    const double per_term = 2.0 * na + 0.75 + (dd ? 1.0 : 0.0);
+    const double per_unit = 12.0 * na + 2.0 * (n - na) + 14.0 * flip + 40.0 + (dd ? 6.0 * na + 60.0 : 0.0);
+    return units * (terms * per_term + per_unit);
 }
 
 struct Choice {
@@ -76,7 +80,7 @@ struct Choice {
 // then lower index), and price every prefix length w.  High columns are
 // ordered by ascending count of nonzeros outside the union, since the Gray
 // code flips high column j once every 2^(j+1) units.
-void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, Choice* best)
+void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, bool dd, Choice* best)
 {
     const int wmax = std::min(10, n - 1 - min_ntop);
     for (int last = 0; last < n; ++last) {
@@ -104,7 +108,7 @@ void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, Choi
                              [&](int x, int y) { return popc(cm[x] & ~U) < popc(cm[y] & ~U); });
             double flip = 0.0;
             for (size_t j = 0; j < high.size(); ++j) flip += std::ldexp((double)popc(cm[high[j]] & ~U), -(int)j - 1);
-            const double cost = walk_cost(n, w, na, flip);
+            const double cost = walk_cost(n, w, na, flip, dd);
             if (cost < best->cost) {
                 best->cost = cost;
                 best->na = na;
@@ -135,10 +139,11 @@ bool plan_compacted(const double* a, int n, int mode, const spb_options& opt, Ch
         if (cm[c] == 0ull) return false;  // zero column: the dense walk returns 0
     }
     const int min_ntop = mode == SPB_SPARSE_WALK_ALWAYS ? std::min(14, n - 3) : 14;
-    choose(cm, n, min_ntop, ch);
+    const bool dd = opt.precision == SPB_PREC_DD;
+    choose(cm, n, min_ntop, dd, ch);
     if (ch->na <= 0) return false;
     const int wd = choose_unit_bits(n, 1, &opt);
-    return mode == SPB_SPARSE_WALK_ALWAYS || ch->cost < 0.8 * walk_cost(n, wd, n, 0.0);
+    return mode == SPB_SPARSE_WALK_ALWAYS || ch->cost < 0.8 * walk_cost(n, wd, n, 0.0, dd);
 }
 
 }  // namespace

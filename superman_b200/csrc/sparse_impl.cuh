@@ -84,15 +84,15 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
     const int ntop = n - 1 - w, ni = n - NA;
     const int tid = threadIdx.x, bd = blockDim.x;
     double* s_de = smem;                   // [nq][NA][4] active rows of DE
-    double* s_ma = s_de + terms * NA;      // [ntop][NA] active part of the high columns
+    double2* s_bnd = reinterpret_cast<double2*>(s_de + terms * NA);  // [NA] DE range (min, max)
+    double* s_ma = reinterpret_cast<double*>(s_bnd + NA);  // [ntop][NA] active part of the high columns
     double* s_iv = s_ma + ntop * NA;       // [ntop][ni] inactive nonzeros, compacted per column
     double* s_lo = s_iv + ntop * ni;       // [NA][bd] active lo words
     double* s_ih = s_lo + NA * bd;         // [ni][bd] inactive hi words
     double* s_il = s_ih + ni * bd;         // [ni][bd] inactive lo words
     double* s_hist = s_il + ni * bd;       // mode 1
     unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
-    double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);  // [2][NA]
-    unsigned char* s_ir = reinterpret_cast<unsigned char*>(s_bnd + 2 * NA);  // [ntop][ni]
+    unsigned char* s_ir = reinterpret_cast<unsigned char*>(s_cnt + kHistBins);  // [ntop][ni]
     unsigned char* s_ic = s_ir + ntop * ni;                                   // [ntop]
 
     for (int i = tid; i < terms * NA; i += bd) {
@@ -114,10 +114,7 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
     }
     const int mode = pb.mode;
     if (mode != 0)
-        for (int r = tid; r < NA; r += bd) {
-            s_bnd[r] = pb.bnd[r];
-            s_bnd[NA + r] = pb.bnd[n + r];
-        }
+        for (int r = tid; r < NA; r += bd) s_bnd[r] = make_double2(pb.bnd[r], pb.bnd[n + r]);
     if (mode == 1)
         for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
     __syncthreads();
@@ -159,8 +156,10 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
             if (mode != 0) {
                 double ub = fabs(c);
 #pragma unroll
-                for (int r = 0; r < NA; ++r)
-                    ub = mul_rn(ub, fmax(fabs(add_rn(xa[r], s_bnd[r])), fabs(add_rn(xa[r], s_bnd[NA + r]))));
+                for (int r = 0; r < NA; ++r) {
+                    const double2 bb = s_bnd[r];
+                    ub = mul_rn(ub, fmax(fabs(add_rn(xa[r], bb.x)), fabs(add_rn(xa[r], bb.y))));
+                }
                 b = hist_bin(ub);
                 bmax = b > bmax ? b : bmax;
                 if (mode == 2 && b >= pb.thr_bin) {

@@ -67,3 +67,30 @@ def test_dd_forced_refinement_signed(spb, oracle):
     r = spb.perm_dense(a, precision="dd", rel_tol=1e-15)
     assert r.refined_units > 0
     assert oracle.rel_err(r.permanent, exact) <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["dense_u01_n24_s3", "dense_u01_n32_s7"])
+def test_dd_listing_paths_agree(spb, oracle, name):
+    """The first pass's unit list and the replay scan select the same units;
+    the results agree to far below the tolerance."""
+    a, exact, _ = load_golden(name)
+    r1 = spb.perm_dense(a, precision="dd")
+    r2 = spb.perm_dense(a, precision="dd", replay_listing=1)
+    assert r1.refined_units == r2.refined_units
+    assert r2.launches > 0 and oracle.rel_err(r2.permanent, exact) <= REL_TOL_DD
+    assert abs((r1.permanent + r1.permanent_lo) - (r2.permanent + r2.permanent_lo)) <= 1e-15 * abs(r1.permanent)
+
+
+def test_dd_parallel_scan_signed(spb, oracle):
+    """Many units to refine (tight tolerance, signed entries): the threshold
+    falls below the first pass's list, so the parallel scan lists them; the
+    replay scan must select the same units."""
+    import numpy as np
+    rng = np.random.default_rng(21)
+    a = rng.standard_normal((22, 22))
+    exact = oracle.exact_perm(a)
+    r1 = spb.perm_dense(a, precision="dd", rel_tol=1e-16)
+    r2 = spb.perm_dense(a, precision="dd", rel_tol=1e-16, replay_listing=1)
+    assert r1.refined_units == r2.refined_units > 0
+    assert oracle.rel_err(r1.permanent, exact) <= 1e-12
+    assert oracle.rel_err(r2.permanent, exact) <= 1e-12

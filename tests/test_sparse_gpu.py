@@ -65,6 +65,10 @@ def test_sparse_dd_refinement_signed(spb, oracle):
     r = spb.perm_sparse(a, precision="dd", rel_tol=1e-15, walk="always")
     assert r.active_rows < 22 and r.refined_units > 0
     assert oracle.rel_err(r.permanent, exact) <= 1e-12
+    # the replay scan (the walk's own unit bases) selects the same units
+    r2 = spb.perm_sparse(a, precision="dd", rel_tol=1e-15, walk="always", replay_listing=1)
+    assert r2.refined_units == r.refined_units
+    assert oracle.rel_err(r2.permanent, exact) <= 1e-12
 
 
 def test_sparse_csc_input_matches_dense_input(spb):
