@@ -77,19 +77,34 @@ __device__ __forceinline__ int hist_bin(double u)
 }
 
 // Shared memory the histogram needs (reserved in every mode so the walk and
-// the scan run with the same launch shape, hence the same unit split).
-constexpr size_t kHistSmemBytes = kHistBins * (sizeof(double) + sizeof(unsigned long long));
+// the scan run with the same launch shape, hence the same unit split).  Per
+// bin: the sum of squared terms as a float scaled by 2^(-8(b-256)) (bin b
+// holds bounds below 2^(4(b-256)+4), so a unit adds at most 2^(w+8)), and a
+// 32-bit count; both have native shared-memory atomics.
+constexpr size_t kHistSmemBytes = kHistBins * (sizeof(float) + sizeof(unsigned));
 // Shared memory for the per-row bound terms (two per row, real or complex).
 __host__ __device__ constexpr size_t bound_smem_bytes(int n) { return sizeof(double) * 2 * n; }
 
-// Per-thread cache of the histogram: consecutive Gray units of one thread
-// usually fall in the same bin, so shared-memory atomics are issued only when
-// the bin changes.
+// 2^(4(b-256)) for bins 1..511 (bin 0 holds zero bounds, whose terms are 0),
+// built from the exponent field; the histogram scale is its square.
+__device__ __forceinline__ double hist_half_scale(int bin)
+{
+    const int b = bin < 1 ? 1 : bin;
+    return __hiloint2double((1023 + 4 * (b - 256)) << 20, 0);
+}
+__device__ __forceinline__ double hist_half_unscale(int bin)
+{
+    const int b = bin < 1 ? 1 : bin;
+    return __hiloint2double((1023 - 4 * (b - 256)) << 20, 0);
+}
+
+// Per-thread cache of the histogram: shared-memory atomics are issued only
+// when a thread's bin changes from one unit to the next.
 struct HistCache {
     int bin = -1;
     double s2 = 0.0;
-    unsigned long long cnt = 0;
-    __device__ __forceinline__ void add(int b, double v, double* s_hist, unsigned long long* s_cnt)
+    unsigned cnt = 0;
+    __device__ __forceinline__ void add(int b, double v, float* s_hist, unsigned* s_cnt)
     {
         if (b != bin) {
             flush(s_hist, s_cnt);
@@ -98,10 +113,11 @@ struct HistCache {
         s2 += v;
         ++cnt;
     }
-    __device__ __forceinline__ void flush(double* s_hist, unsigned long long* s_cnt)
+    __device__ __forceinline__ void flush(float* s_hist, unsigned* s_cnt)
     {
         if (cnt) {
-            atomicAdd(&s_hist[bin], s2);
+            const double h = hist_half_unscale(bin);
+            atomicAdd(&s_hist[bin], __double2float_rn((s2 * h) * h));
             atomicAdd(&s_cnt[bin], cnt);
         }
         s2 = 0.0;
@@ -109,14 +125,14 @@ struct HistCache {
     }
 };
 
-// Flushes a CTA's shared histogram into the global one.
-__device__ __forceinline__ void flush_hist(const double* s_hist, const unsigned long long* s_cnt,
-                                           const Problem& pb)
+// Flushes a CTA's shared histogram into the global one (double, 64-bit).
+__device__ __forceinline__ void flush_hist(const float* s_hist, const unsigned* s_cnt, const Problem& pb)
 {
     for (int i = threadIdx.x; i < kHistBins; i += blockDim.x)
         if (s_cnt[i]) {
-            atomicAdd(&pb.hist_cnt[i], s_cnt[i]);
-            atomicAdd(&pb.hist_s2[i], s_hist[i]);
+            atomicAdd(&pb.hist_cnt[i], (unsigned long long)s_cnt[i]);
+            const double h = hist_half_scale(i);
+            atomicAdd(&pb.hist_s2[i], ((double)s_hist[i] * h) * h);
         }
 }
 
@@ -258,8 +274,8 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     double* s_de = smem;
     double* s_mt = s_de + terms * N;
     double* s_lo = s_mt + (ntop > 0 ? ntop : 0) * N;
-    double* s_hist = s_lo + N * bd;  // mode 1
-    unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
+    float* s_hist = reinterpret_cast<float*>(s_lo + N * bd);  // mode 1
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
     // DE range per row, [2][N] (min, max).  Two scalar loads per row: a paired
     // 16-byte load keeps more registers live and makes the n=32 walk spill.
     double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);
@@ -269,7 +285,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     if (mode != 0)
         for (int i = tid; i < 2 * N; i += bd) s_bnd[i] = pb.bnd[i];
     if (mode == 1)
-        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
     __syncthreads();
 
     const unsigned long long T = (unsigned long long)gridDim.x * bd;
@@ -425,8 +441,8 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     double* s_de = smem;                        // [2][terms*N]
     double* s_mt = s_de + 2 * terms * N;        // [2][ntop*N]
     double* s_lo = s_mt + 2 * ntp * N;          // [2][N][bd]
-    double* s_hist = s_lo + 2 * N * bd;         // mode 1
-    unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
+    float* s_hist = reinterpret_cast<float*>(s_lo + 2 * N * bd);  // mode 1
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
     double* s_bnd = reinterpret_cast<double*>(s_cnt + kHistBins);  // [N]
     for (int i = tid; i < 2 * terms * N; i += bd) s_de[i] = pb.de_hi[i];
     for (int i = tid; i < 2 * ntp * N; i += bd) s_mt[i] = pb.mt[i];
@@ -434,7 +450,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     if (mode != 0)
         for (int i = tid; i < N; i += bd) s_bnd[i] = pb.bnd[i];
     if (mode == 1)
-        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
     __syncthreads();
     const double* s_mt_re = s_mt;
     const double* s_mt_im = s_mt + ntp * N;

@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
     double* s_lo = s_iv + ntop * ni;       // [NA][bd] active lo words
     double* s_ih = s_lo + NA * bd;         // [ni][bd] inactive hi words
     double* s_il = s_ih + ni * bd;         // [ni][bd] inactive lo words
-    double* s_hist = s_il + ni * bd;       // mode 1
-    unsigned long long* s_cnt = reinterpret_cast<unsigned long long*>(s_hist + kHistBins);
+    float* s_hist = reinterpret_cast<float*>(s_il + ni * bd);  // mode 1
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
     unsigned char* s_ir = reinterpret_cast<unsigned char*>(s_cnt + kHistBins);  // [ntop][ni]
     unsigned char* s_ic = s_ir + ntop * ni;                                   // [ntop]
 
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
     if (mode != 0)
         for (int r = tid; r < NA; r += bd) s_bnd[r] = make_double2(pb.bnd[r], pb.bnd[n + r]);
     if (mode == 1)
-        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0; s_cnt[i] = 0ull; }
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
     __syncthreads();
 
     const unsigned long long T = (unsigned long long)gridDim.x * bd;
