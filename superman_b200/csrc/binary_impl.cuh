@@ -174,11 +174,11 @@ __global__ void __launch_bounds__(bin_max_threads(N), 1) walk_binary(Problem pb)
         int xt[N];
         const unsigned long long g0 = gray_of(u0);
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-            int x = 0;
-            for (int j = 0; j < ntop; ++j)
-                if ((g0 >> j) & 1ull) x += s_mt[j * N + r];
-            xt[r] = x;
+        for (int r = 0; r < N; ++r) xt[r] = 0;
+        for (int j = 0; j < ntop; ++j) {  // columns outermost, rows independent
+            if (!((g0 >> j) & 1ull)) continue;
+#pragma unroll
+            for (int r = 0; r < N; ++r) xt[r] += s_mt[j * N + r];
         }
         unsigned long long u = u0;
         while (true) {

@@ -63,12 +63,14 @@ __global__ void __launch_bounds__(256) bound_walk(Problem pb)
 #pragma unroll
     for (int c = 0; c < C; ++c)
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-            float v = (float)pb.x0_hi[c * N + r];
-            for (int j = 0; j < ntop; ++j)
-                if ((g0 >> j) & 1ull) v += s_mt[(c * ntp + j) * N + r];
-            x[c][r] = C == 1 ? v + s_b[r] : v;  // real: y_r = x_r + mid_r
-        }
+        for (int r = 0; r < N; ++r) x[c][r] = (float)pb.x0_hi[c * N + r] + (C == 1 ? s_b[r] : 0.0f);  // real: y = x + mid
+    for (int j = 0; j < ntop; ++j) {  // columns outermost, rows independent
+        if (!((g0 >> j) & 1ull)) continue;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+#pragma unroll
+            for (int r = 0; r < N; ++r) x[c][r] += s_mt[(c * ntp + j) * N + r];
+    }
 #pragma unroll
     for (int r = 0; r < N; ++r) hb[r] = C == 1 ? s_b[N + r] : s_b[r];
     for (unsigned long long u = u0; u < u1; ++u) {
@@ -86,7 +88,10 @@ __global__ void __launch_bounds__(256) bound_walk(Problem pb)
         for (int r = 0; r < N; ++r) {
             float f;
             if constexpr (C == 1) f = fabsf(x[0][r]) + hb[r];
-            else f = sqrtf(fmaf(x[0][r], x[0][r], x[C - 1][r] * x[C - 1][r])) + hb[r];
+            else {
+                const float m2 = fmaxf(fmaf(x[0][r], x[0][r], x[C - 1][r] * x[C - 1][r]), 0x1p-100f);
+                f = m2 * rsqrtf(m2) + hb[r];  // |x| to a few ulps: an estimate
+            }
             p *= fminf(fmaxf(f, 0x1p-24f), 0x1p24f);
             if ((r & 3) == 3) bound_renorm(p, e);
         }

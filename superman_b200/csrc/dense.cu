@@ -89,9 +89,13 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
     }
     // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
     //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|.
+    //     The complex maximum spreads the (row, d) pairs over all threads; the
+    //     bit patterns of non-negative doubles order like the values.
+    __shared__ unsigned long long s_bmax[kMaxN];
+    for (int r = tid; r < n; r += bd) s_bmax[r] = 0ull;
     __syncthreads();  // the complex bound reads the table written above
-    for (int r = tid; r < n; r += bd) {
-        if (c == 1) {
+    if (c == 1) {
+        for (int r = tid; r < n; r += bd) {
             double lo = 0.0, hi = 0.0;
             for (int j = 0; j < w; ++j) {
                 double v = pb.as[(size_t)r * n + j];
@@ -99,14 +103,16 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
             }
             pb.bnd[r] = lo;
             pb.bnd[n + r] = hi;
-        } else {
-            double m = 0.0;
-            for (int d = 0; d < terms; ++d) {
-                size_t pos = ((size_t)(d / G) * n + r) * G + (d % G);
-                m = fmax(m, hypot(pb.de_hi[pos], pb.de_hi[(size_t)terms * n + pos]));
-            }
-            pb.bnd[r] = m * (1.0 + 0x1p-50);
         }
+    } else {
+        for (int idx = tid; idx < terms * n; idx += bd) {
+            const int r = idx % n, d = idx / n;
+            const size_t pos = ((size_t)(d / G) * n + r) * G + (d % G);
+            const double m = hypot(pb.de_hi[pos], pb.de_hi[(size_t)terms * n + pos]);
+            atomicMax(&s_bmax[r], (unsigned long long)__double_as_longlong(m));
+        }
+        __syncthreads();
+        for (int r = tid; r < n; r += bd) pb.bnd[r] = __longlong_as_double((long long)s_bmax[r]) * (1.0 + 0x1p-50);
     }
     // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
     const int ntop = n - 1 - w;

@@ -301,6 +301,10 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     if (u0 < u1) {
         double xh[N];
         const unsigned long long g0 = gray_of(u0);
+        // First unit base: x0 plus the selected high columns in index order
+        // (the refinement's rebuild does the same).  Row by row: with the
+        // column loop outermost the compiler keeps every row's lo word live
+        // and the walk spills.
 #pragma unroll
         for (int r = 0; r < N; ++r) {
             dd x = {pb.x0_hi[r], pb.x0_lo[r]};

@@ -368,8 +368,11 @@ int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s)
 {
     const int threads = 256;
     const size_t smem = bound_smem_bytes_f(pb.n, pb.comps, pb.w);
-    blocks *= 2;  // two CTAs per SM
-    unsigned long long max_blocks = (pb.units + threads - 1) / threads;
+    // Two CTAs per SM, but at least 8 units per thread: a thread's first
+    // unit base costs n*(n-1-w) adds, so few units per thread would be
+    // dominated by that start.
+    blocks *= 2;
+    unsigned long long max_blocks = (pb.units + 8ull * threads - 1) / (8ull * threads);
     if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
     if (blocks < 1) blocks = 1;
     int st = SPB_ERR_INVALID;
