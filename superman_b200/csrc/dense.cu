@@ -139,7 +139,7 @@ namespace dense {
 int group_size(int n, int comps)
 {
     if (comps == 1) return n >= 3 ? 4 : (n == 2 ? 2 : 1);
-    return n >= 2 ? 2 : 1;
+    return ComplexGroup(n);
 }
 
 int choose_unit_bits(int n, int comps, const spb_options* opt)

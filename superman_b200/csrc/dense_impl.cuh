@@ -140,7 +140,7 @@ __device__ __forceinline__ void flush_hist(const float* s_hist, const unsigned* 
 // chains under the per-thread register budget the cap implies
 // (65536 / threads), so the walk never spills at the sizes that matter.
 __host__ __device__ constexpr int RealMaxThreads(int n) { return n <= 40 ? 512 : 256; }
-__host__ __device__ constexpr int ComplexMaxThreads(int n) { return n <= 14 ? 512 : (n <= 26 ? 384 : 256); }
+__host__ __device__ constexpr int ComplexMaxThreads(int n) { return n <= 10 ? 512 : (n <= 20 ? 384 : 256); }
 
 template <int N>
 struct RealCfg {
@@ -148,9 +148,13 @@ struct RealCfg {
     static constexpr int kMaxThreads = RealMaxThreads(N);
 };
 
+// Complex groups: four independent term chains per component while the
+// x vector leaves room for them in registers (n <= 32), two beyond.
+__host__ __device__ constexpr int ComplexGroup(int n) { return (n >= 3 && n <= 32) ? 4 : (n >= 2 ? 2 : 1); }
+
 template <int N>
 struct ComplexCfg {
-    static constexpr int G = N >= 2 ? 2 : 1;
+    static constexpr int G = ComplexGroup(N);
     static constexpr int kMaxThreads = ComplexMaxThreads(N);
 };
 
@@ -391,7 +395,14 @@ __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const do
 #pragma unroll
         for (int r = 1; r < N; ++r) {
             double vr[G], vi[G];
-            if constexpr (G == 2) {
+            if constexpr (G == 4) {
+                double2 a0 = reinterpret_cast<const double2*>(dr + r * 4)[0];
+                double2 a1 = reinterpret_cast<const double2*>(dr + r * 4)[1];
+                double2 b0 = reinterpret_cast<const double2*>(di + r * 4)[0];
+                double2 b1 = reinterpret_cast<const double2*>(di + r * 4)[1];
+                vr[0] = a0.x; vr[1] = a0.y; vr[2] = a1.x; vr[3] = a1.y;
+                vi[0] = b0.x; vi[1] = b0.y; vi[2] = b1.x; vi[3] = b1.y;
+            } else if constexpr (G == 2) {
                 double2 a = reinterpret_cast<const double2*>(dr + r * 2)[0];
                 double2 b = reinterpret_cast<const double2*>(di + r * 2)[0];
                 vr[0] = a.x; vr[1] = a.y; vi[0] = b.x; vi[1] = b.y;
@@ -412,7 +423,10 @@ __device__ __forceinline__ void unit_sum_complex(const double (&xr)[N], const do
             }
         }
         double gr, gi;
-        if constexpr (G == 2) { gr = sub_rn(pr[0], pr[1]); gi = sub_rn(pi[0], pi[1]); }
+        if constexpr (G == 4) {  // + - - +
+            gr = sub_rn(sub_rn(pr[0], pr[1]), sub_rn(pr[2], pr[3]));
+            gi = sub_rn(sub_rn(pi[0], pi[1]), sub_rn(pi[2], pi[3]));
+        } else if constexpr (G == 2) { gr = sub_rn(pr[0], pr[1]); gi = sub_rn(pi[0], pi[1]); }
         else { gr = pr[0]; gi = pi[0]; }
         if (__popc(q) & 1) { ar = sub_rn(ar, gr); ai = sub_rn(ai, gi); }
         else { ar = add_rn(ar, gr); ai = add_rn(ai, gi); }

@@ -61,12 +61,12 @@ __device__ __forceinline__ double group_sum_real_rt(const double* xh, const doub
     return p0;
 }
 
-// One group of G (<= 2) complex terms, bitwise identical to unit_sum_complex<N,G>.
+// One group of G (<= 4) complex terms, bitwise identical to unit_sum_complex<N,G>.
 __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const double* xi,
                                                      const double* dr, const double* di, int n,
                                                      int G, double& gr, double& gi)
 {
-    double pr[2] = {0.0, 0.0}, pi[2] = {0.0, 0.0};
+    double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = 0; i < G; ++i) {
         pr[i] = add_rn(xr[0], dr[i]);
         pi[i] = add_rn(xi[0], di[i]);
@@ -83,7 +83,10 @@ __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const dou
             pi[i] = ni;
         }
     }
-    if (G == 2) {
+    if (G == 4) {
+        gr = sub_rn(sub_rn(pr[0], pr[1]), sub_rn(pr[2], pr[3]));
+        gi = sub_rn(sub_rn(pi[0], pi[1]), sub_rn(pi[2], pi[3]));
+    } else if (G == 2) {
         gr = sub_rn(pr[0], pr[1]);
         gi = sub_rn(pi[0], pi[1]);
     } else {
