@@ -6,9 +6,10 @@
 //    sparse route (the reference's code-generation algorithms);
 //  * any sparse-style algorithm, or a non-register algorithm on a matrix
 //    below 30 % density, takes the sparse driver.
+//  * "approximation" takes the sampling driver (gpuApproxSingleGPU).
 // This library computes on one GPU only: mode=cpu and the multi-GPU modes
 // are reported as unavailable (the reference's own error for modes it was
-// not built with), and the Monte-Carlo approximation is not provided.
+// not built with).
 #pragma once
 
 #include <stdexcept>
@@ -28,8 +29,7 @@ public:
         if (settings->mode != SingleGPU)
             throw std::runtime_error(
                 "The mode you want to calculate the permanent in is unavailable for launch. Terminating...\n");
-        if (settings->algorithm == APPROXIMATION)
-            throw std::runtime_error("The approximation algorithm is not provided by superman_b200.\n");
+        if (settings->algorithm == APPROXIMATION) return &gpuApproxSingleGPU<C, S>;
         if (settings->algorithm == AlgorithmEnds) {
             const bool dense = (matrix->nov * matrix->sparsity / 100 <= 6) || (biggestComponentSize <= 41) ||
                                ((int)biggestComponentSize <= matrix->nov - 3);

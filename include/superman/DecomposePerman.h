@@ -78,6 +78,12 @@ private:
 
     void startRecursion(Matrix<S>* m)
     {
+        // The approximation samples the whole matrix as one piece
+        // (CommonFiles/DecomposePerman.h:122-126).
+        if (m_Settings.algorithm == APPROXIMATION) {
+            enqueue(m);
+            return;
+        }
         bool folded = true;
         while (folded && m->nov > kFoldAbove) {
             folded = fold1(m) || fold2(m);
@@ -111,7 +117,7 @@ private:
     void enqueue(Matrix<S>* m)
     {
         m->sparsity = m->nov ? 100.0 * getNNZ(m) / ((double)m->nov * m->nov) : 0.0;
-        if (m->nov > 63)
+        if (m->nov > 63 && m_Settings.algorithm != APPROXIMATION)
             throw std::runtime_error("Permanent is an #P-complete problem. The size of the matrix you want to calculate the permanent for exceeds the limit of what is computationally possible. Try approximation algorithms.\n");
         std::unique_ptr<ScalingCompact> sc;
         if (m_Settings.scaling) {

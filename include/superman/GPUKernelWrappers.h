@@ -117,6 +117,42 @@ protected:
     }
 };
 
+// Sampling driver, the reference's aspSingleGPU (Algorithms/GPU/Sparse/
+// aspSingleGPU.cuh:45-165): rows sorted by degree and the sparse layout
+// built as the reference's Permanent::computePermanent does for the
+// approximation (CommonFiles/Permanent.h:76-81), then spb_perm_approx on the
+// pattern.  Sample count and seed: Settings::approxSamples (default 1e8, the
+// reference's NO_SAMPLES) and Settings::approxSeed.
+template <class C, class S>
+class spbApproxSingleGPU : public Permanent<C, S> {
+public:
+    spbApproxSingleGPU(Matrix<S>* matrix, Settings settings) : Permanent<C, S>(matrix, settings) {}
+    double permanentFunction() final
+    {
+        auto* sp = dynamic_cast<SparseMatrix<S>*>(this->m_Matrix);
+        if (!sp) throw std::runtime_error("superman_b200: the approximation driver needs its sparse layout\n");
+        spb_options o = spb_detail::options_from(this->m_Settings);
+        spb_result r;
+        spb_detail::check(spb_perm_approx(sp->cptrs, sp->rows, sp->nov, this->m_Settings.approxSamples,
+                                          this->m_Settings.approxSeed, &o, &r));
+        return r.value;
+    }
+
+protected:
+    void prepare() override
+    {
+        IO::rowSort(this->m_Matrix);
+        this->m_Matrix = new SparseMatrix<S>(this->m_Matrix, getNNZ(this->m_Matrix));
+    }
+};
+
+template <class C, class S>
+Result gpuApproxSingleGPU(Matrix<S>* matrix, Settings* settings)
+{
+    DecomposePerman<C, S, spbApproxSingleGPU<C, S>> d(matrix, *settings);
+    return d.computePermanentRecursively();
+}
+
 template <class C, class S>
 Result gpuDPSingleGPU(Matrix<S>* matrix, Settings* settings)
 {

@@ -176,6 +176,8 @@ public:
             else if (k == "undirected") s.undirected = v == "true";
             else if (k == "scaling") s.scaling = v == "true";
             else if (k == "scaling_iteration_no") s.scalingIterationNo = (unsigned)toInt(v, "scaling_iteration_no");
+            else if (k == "approx_samples") s.approxSamples = toU64(v, "approx_samples");
+            else if (k == "approx_seed") s.approxSeed = toU64(v, "approx_seed");
             else if (k == "scale_into") s.scaleInto = (unsigned)toInt(v, "scale_into");
             else if (k == "calculation_precision") {
                 if (v == "kahan") s.calculationPrecision = KAHAN;
@@ -235,6 +237,15 @@ private:
     {
         try {
             return std::stoi(v);
+        } catch (const std::exception&) {
+            throw std::runtime_error(std::string("An integer value should be provided to the ") + key + " argument!\n");
+        }
+    }
+
+    static unsigned long long toU64(const std::string& v, const char* key)
+    {
+        try {
+            return std::stoull(v);
         } catch (const std::exception&) {
             throw std::runtime_error(std::string("An integer value should be provided to the ") + key + " argument!\n");
         }

@@ -50,4 +50,10 @@ struct Settings {
 
     int rank = 0;
     int processorNum = 1;
+
+    // Approximation (algorithm=approximation): number of samples (the
+    // reference's NO_SAMPLES, Algorithms/GPU/GPUHelpers.cuh:39) and the seed
+    // of the sample streams.  Keys approx_samples= and approx_seed=.
+    unsigned long long approxSamples = 100000000ull;
+    unsigned long long approxSeed = 1ull;
 };

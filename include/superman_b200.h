@@ -135,6 +135,26 @@ SPB_API int spb_perm_sparse_f64(const int* cptrs, const int* rows, const double*
  * na..n-1 are zero in columns 0..w-1.  CPU only. */
 SPB_API int spb_sparse_plan(const double* a, int n, int mode, int* na, int* w, int* row_order, int* col_order);
 
+/* Monte-Carlo estimate of the permanent of the nonzero pattern of an n x n
+ * matrix (its number of perfect matchings; the values are not used), for
+ * any n up to 2^20 — beyond the exact paths' n <= 63.  Replaces aspSingleGPU
+ * (Algorithms/GPU/Sparse/aspSingleGPU.cuh:45-165) with its kernel
+ * rasmussenScaleAB (Algorithms/GPU/Sparse/ApproximateSparseKernelDefinitions.cuh:
+ * 177-290): sequential importance sampling over the rows in order, with the
+ * same host scaling (50 passes), per-row scaling (10 passes) and degree-1
+ * propagation.  The pattern comes as compressed-column arrays (cptrs[n+1],
+ * rows[cptrs[n]]).  `samples` estimates are averaged; sample k draws from its
+ * own stream of `seed`, so the result does not depend on the launch shape.
+ * out->value is the mean, out->err_est the standard error relative to it,
+ * out->gray_steps the number of samples. */
+SPB_API int spb_perm_approx(const int* cptrs, const int* rows, int n, uint64_t samples, uint64_t seed,
+                            const spb_options* opt, spb_result* out);
+
+/* The individual estimates of samples first .. first+count-1 of
+ * spb_perm_approx (same pattern, same seed), into estimates[count] (host). */
+SPB_API int spb_approx_samples(const int* cptrs, const int* rows, int n, uint64_t first, uint64_t count,
+                               uint64_t seed, double* estimates);
+
 /* Same on a device-resident row-major matrix. */
 SPB_API int spb_perm_dense_f64_dev(const double* d_a, int n, const spb_options* opt,
                            spb_result* out);

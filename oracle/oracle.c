@@ -569,3 +569,134 @@ void orc_perm_mod_primes_gauss(const uint64_t* kre, const uint64_t* kim, int n,
     }
     free(ktr); free(kti); free(x0r); free(x0i); free(br); free(bi); free(pr_); free(pi_);
 }
+
+/* ------------------------------------------------------------------------
+ * Sequential importance sampling (aspSingleGPU / rasmussenScaleAB,
+ * Algorithms/GPU/Sparse/ApproximateSparseKernelDefinitions.cuh:32-290).
+ * ---------------------------------------------------------------------- */
+void orc_rasmussen_init(int n, const int* rptr, const int* col, const int* cptr, const int* row,
+                        float* rv, float* cv)
+{
+    for (int i = 0; i < n; ++i) rv[i] = cv[i] = 1.0f;
+    for (int it = 0; it < 50; ++it) {  /* ApproximateSparseKernelDefinitions.cuh:32-61 */
+        for (int j = 0; j < n; ++j) {
+            float s = 0.0f;
+            for (int q = cptr[j]; q < cptr[j + 1]; ++q) s = s + rv[row[q]];
+            cv[j] = 1.0f / s;
+        }
+        for (int i = 0; i < n; ++i) {
+            float s = 0.0f;
+            for (int p = rptr[i]; p < rptr[i + 1]; ++p) s = s + cv[col[p]];
+            rv[i] = 1.0f / s;
+        }
+    }
+}
+
+static uint64_t orc_splitmix(uint64_t* s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* :124-172: removal of line `start` (a column when by_col) lowers the entry
+ * counts of the crossing lines still present; a crossing line left with one
+ * entry is matched to it; none left: no perfect matching (returns 1). */
+static int orc_propagate(const int* optr, const int* oidx, const int* sptr, const int* sidx,
+                         float* so, float* ss, int* cnt, int* stk, int start)
+{
+    int sp = 1;
+    stk[0] = start;
+    for (int ii = 0; ii < sp; ++ii) {
+        const int j = stk[ii];
+        for (int q = optr[j]; q < optr[j + 1]; ++q) {
+            const int i = oidx[q];
+            if (so[i] == 0.0f) continue;
+            const int k = --cnt[i];
+            if (k == 0) return 1;
+            if (k != 1) continue;
+            for (int p = sptr[i]; p < sptr[i + 1]; ++p) {
+                const int j2 = sidx[p];
+                if (ss[j2] == 0.0f) continue;
+                so[i] = 0.0f;
+                ss[j2] = 0.0f;
+                stk[sp++] = j2;
+                break;
+            }
+        }
+    }
+    return 0;
+}
+
+static double orc_rasmussen_one(int n, const int* rptr, const int* col, const int* cptr, const int* row,
+                                const float* rv0, const float* cv0, uint64_t seed, uint64_t k,
+                                float* rv, float* cv, int* re, int* ce, int* stk)
+{
+    for (int i = 0; i < n; ++i) {
+        re[i] = rptr[i + 1] - rptr[i];
+        ce[i] = cptr[i + 1] - cptr[i];
+        rv[i] = rv0[i];
+        cv[i] = cv0[i];
+    }
+    uint64_t rng = seed ^ (k * 0xD1B54A32D192ED03ull);
+    double est = 1.0;
+    for (int i = 0; i < n; ++i) {
+        for (int it = 0; it < 10; ++it) {  /* scaleAB, :63-122 */
+            for (int p = rptr[i]; p < rptr[i + 1]; ++p) {
+                const int j = col[p];
+                if (cv[j] == 0.0f) continue;
+                float s = 0.0f;
+                for (int q = cptr[j]; q < cptr[j + 1]; ++q) s = s + rv[row[q]];
+                if (s == 0.0f) return 0.0;
+                cv[j] = 1.0f / s;
+            }
+            if (rv[i] != 0.0f) {
+                float s = 0.0f;
+                for (int p = rptr[i]; p < rptr[i + 1]; ++p) s = s + cv[col[p]];
+                if (s == 0.0f) return 0.0;
+                rv[i] = 1.0f / s;
+            }
+        }
+        const float ri = rv[i];
+        if (ri == 0.0f) continue;
+        const float u = (float)((orc_splitmix(&rng) >> 40) + 1ull) * 0x1p-24f;
+        float run = 0.0f, prob = 0.0f;
+        int chosen = -1;
+        for (int p = rptr[i]; p < rptr[i + 1]; ++p) {  /* :246-259 */
+            const int j = col[p];
+            const float cj = cv[j];
+            if (cj == 0.0f) continue;
+            prob = ri * cj;
+            run = run + prob;
+            chosen = j;
+            if (run > u) break;
+        }
+        if (chosen < 0) return 0.0;
+        est = est * (1.0 / (double)prob);
+        rv[i] = 0.0f;
+        cv[chosen] = 0.0f;
+        if (orc_propagate(cptr, row, rptr, col, rv, cv, re, stk, chosen) ||
+            orc_propagate(rptr, col, cptr, row, cv, rv, ce, stk, i))
+            return 0.0;
+    }
+    return est;
+}
+
+void orc_rasmussen_samples(int n, const int* rptr, const int* col, const int* cptr, const int* row,
+                           const float* rv0, const float* cv0, uint64_t seed, uint64_t first,
+                           uint64_t count, int threads, double* out)
+{
+    if (threads < 1) threads = 1;
+#pragma omp parallel num_threads(threads)
+    {
+        float* rv = (float*)malloc(sizeof(float) * (size_t)n * 2);
+        int* ib = (int*)malloc(sizeof(int) * (size_t)n * 3);
+#pragma omp for schedule(static)
+        for (long long k = 0; k < (long long)count; ++k)
+            out[k] = orc_rasmussen_one(n, rptr, col, cptr, row, rv0, cv0, seed, first + (uint64_t)k, rv, rv + n,
+                                       ib, ib + n, ib + 2 * (size_t)n);
+        free(rv);
+        free(ib);
+    }
+}

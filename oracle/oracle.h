@@ -48,6 +48,25 @@ void orc_perm_mod_primes_gauss(const uint64_t* kre, const uint64_t* kim, int n,
                                const uint64_t* primes, int np, int threads,
                                uint64_t* out_re, uint64_t* out_im);
 
+/* Sequential importance sampling estimate of the number of perfect matchings
+ * of a 0/1 pattern, restating aspSingleGPU / rasmussenScaleAB
+ * (Algorithms/GPU/Sparse/aspSingleGPU.cuh:45-165,
+ * Algorithms/GPU/Sparse/ApproximateSparseKernelDefinitions.cuh:32-290): host
+ * scaling (50 alternating column/row passes), then per sample and per row in
+ * order 10 scaling passes over the row's columns and the row, a draw with
+ * probability rv_i*cv_j, and degree-1 propagation from the removed column
+ * and row.  Pattern in both orientations (rptr/col, cptr/row, indices
+ * ascending, no duplicates).  Sample k draws from SplitMix64 seeded with
+ * seed ^ (k * 0xD1B54A32D192ED03).  Float arithmetic without contraction,
+ * in the same order as the product, so estimates match it bit for bit.
+ * orc_rasmussen_init fills rv[n], cv[n]; orc_rasmussen_samples writes the
+ * estimates of samples first .. first+count-1. */
+void orc_rasmussen_init(int n, const int* rptr, const int* col, const int* cptr, const int* row,
+                        float* rv, float* cv);
+void orc_rasmussen_samples(int n, const int* rptr, const int* col, const int* cptr, const int* row,
+                           const float* rv0, const float* cv0, uint64_t seed, uint64_t first,
+                           uint64_t count, int threads, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,13 @@ def lib() -> ctypes.CDLL:
     L.orc_perm_mod_primes_gauss.restype = None
     L.orc_perm_mod_primes_gauss.argtypes = [u64p, u64p, ctypes.c_int, u64p, ctypes.c_int,
                                             ctypes.c_int, u64p, u64p]
+    ip = ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.orc_rasmussen_init.restype = None
+    L.orc_rasmussen_init.argtypes = [ctypes.c_int, ip, ip, ip, ip, fp, fp]
+    L.orc_rasmussen_samples.restype = None
+    L.orc_rasmussen_samples.argtypes = [ctypes.c_int, ip, ip, ip, ip, fp, fp, ctypes.c_uint64,
+                                        ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, dp]
     return L
 
 
@@ -251,6 +258,31 @@ def exact_perm_complex(a, threads=None):
 
 
 # ------------------------------------------------- pure Python, small n ----
+
+def rasmussen_samples(a, first: int, count: int, seed: int, threads=None):
+    """Estimates of samples first .. first+count-1 of the sequential
+    importance sampler on the nonzero pattern of `a` (orc_rasmussen_samples)."""
+    import numpy as np
+    pat = np.asarray(a) != 0
+    n = pat.shape[0]
+    rptr = np.zeros(n + 1, dtype=np.int32)
+    rptr[1:] = np.cumsum(pat.sum(axis=1))
+    col = np.ascontiguousarray(np.nonzero(pat)[1], dtype=np.int32)
+    cptr = np.zeros(n + 1, dtype=np.int32)
+    cptr[1:] = np.cumsum(pat.sum(axis=0))
+    row = np.ascontiguousarray(np.nonzero(pat.T)[1], dtype=np.int32)
+    L = lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
+    rv = np.zeros(n, dtype=np.float32)
+    cv = np.zeros(n, dtype=np.float32)
+    args = [x.ctypes.data_as(ip) for x in (rptr, col, cptr, row)]
+    L.orc_rasmussen_init(n, *args, rv.ctypes.data_as(fp), cv.ctypes.data_as(fp))
+    out = np.zeros(count)
+    L.orc_rasmussen_samples(n, *args, rv.ctypes.data_as(fp), cv.ctypes.data_as(fp), seed, first, count,
+                            _threads(threads), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
+
 
 def brute_perm(a):
     """Sum over all permutations, exact for int/Fraction entries (n <= 8)."""

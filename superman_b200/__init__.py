@@ -17,8 +17,8 @@ import numpy as np
 from . import _lib
 from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
 
-__all__ = ["Result", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "SupermanError",
-           "SPB_PREC_FP64", "SPB_PREC_DD", "device_count"]
+__all__ = ["Result", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "perm_approx",
+           "approx_samples", "SupermanError", "SPB_PREC_FP64", "SPB_PREC_DD", "device_count"]
 
 _PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD}
 _SPARSE_WALK = {"auto": 0, "never": 1, "always": 2}
@@ -101,6 +101,46 @@ def perm_sparse(a, precision="fp64", device: int = 0, walk: str = "auto", **shap
                                         ctypes.byref(opt), ctypes.byref(out))
     _lib.check(st)
     return _to_result(out, False)
+
+
+def _csc_pattern(a):
+    """(cptrs, rows) of the nonzero pattern of a square matrix, or the
+    pattern part of a (cptrs, rows[, vals]) triple."""
+    if isinstance(a, tuple):
+        return np.ascontiguousarray(a[0], dtype=np.int32), np.ascontiguousarray(a[1], dtype=np.int32)
+    a = np.asarray(a)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("needs a square 2-D array or a compressed-column tuple")
+    c_idx, r_idx = np.nonzero(a.T)
+    cptrs = np.zeros(a.shape[0] + 1, dtype=np.int64)
+    np.add.at(cptrs, c_idx + 1, 1)
+    return np.cumsum(cptrs).astype(np.int32), np.ascontiguousarray(r_idx, dtype=np.int32)
+
+
+def perm_approx(a, samples: int = 1_000_000, seed: int = 1, device: int = 0, **shape) -> Result:
+    """Monte-Carlo estimate of the permanent of the nonzero pattern of `a`
+    (its number of perfect matchings), any n up to 2^20; the mirror of the
+    reference's approximation algorithm.  Result.err_est is the relative
+    standard error of the mean."""
+    cptrs, rows = _csc_pattern(a)
+    out = _lib.spb_result()
+    opt = _lib.default_options(device=device, **shape)
+    ip = ctypes.POINTER(ctypes.c_int)
+    st = _lib.lib().spb_perm_approx(cptrs.ctypes.data_as(ip), rows.ctypes.data_as(ip), cptrs.size - 1,
+                                    samples, seed, ctypes.byref(opt), ctypes.byref(out))
+    _lib.check(st)
+    return _to_result(out, False)
+
+
+def approx_samples(a, first: int, count: int, seed: int = 1) -> np.ndarray:
+    """The individual estimates of samples first .. first+count-1 of
+    perm_approx(a, seed=seed)."""
+    cptrs, rows = _csc_pattern(a)
+    est = np.zeros(count)
+    ip = ctypes.POINTER(ctypes.c_int)
+    _lib.check(_lib.lib().spb_approx_samples(cptrs.ctypes.data_as(ip), rows.ctypes.data_as(ip), cptrs.size - 1,
+                                             first, count, seed, est.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return est
 
 
 def perm_binary(a, device: int = 0, **shape) -> Result:

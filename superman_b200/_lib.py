@@ -128,6 +128,10 @@ SIGNATURES = {
     "spb_sparse_plan": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
+    "spb_perm_approx": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                       ctypes.c_uint64, ctypes.c_uint64, _OP, _RP]),
+    "spb_approx_samples": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                          ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, _DP]),
     "spb_perm_sparse_f64": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _DP,
                                            ctypes.c_int, _OP, _RP]),
     "spb_perm_dense_f64_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _OP, _RP]),

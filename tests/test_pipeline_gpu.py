@@ -71,8 +71,10 @@ def test_pipeline_mode_errors(spb):
     a = W.dense_uniform(5, 1)
     st, _ = pipeline(a, "mode=cpu")
     assert st == _lib.SPB_ERR_INVALID and "unavailable" in _lib.last_error()
-    st, _ = pipeline(a, "algorithm=approximation")
-    assert st == _lib.SPB_ERR_INVALID
+    st, _ = pipeline(a, "algorithm=no_such_algorithm")
+    assert st == _lib.SPB_ERR_INVALID and "UNKNOWN ALGORITHM" in _lib.last_error()
+    st, _ = pipeline(a, "approx_samples=many")
+    assert st == _lib.SPB_ERR_INVALID and "approx_samples" in _lib.last_error()
 
 
 def write_mtx(path, a):
