@@ -218,6 +218,17 @@ def reference_arm(args, wl):
 
 
 # ------------------------------------------------------------- our GPU arm --
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings over the process group (the
+    replicas' job takes as long as its slowest rank); identity on one rank."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def ours_arm(args, wl):
     import numpy as np
     import torch
@@ -283,9 +294,7 @@ def ours_arm(args, wl):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-            t = torch.tensor([total_ms, walk_s], device=f"cuda:{device}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms, walk_s = t[0].item(), t[1].item()
+        total_ms, walk_s = max_over_ranks([total_ms, walk_s], dist, f"cuda:{device}")
         return total_ms / args.steps, walk_s / args.steps, launches
 
     with ClockSampler(device) as clk:
