@@ -32,10 +32,17 @@ struct Cfg {
     static constexpr int TERMS = 1 << W;
     static constexpr int NTOP = N - 1 - W;
     static constexpr int NTP = NTOP > 0 ? NTOP : 0;
-    // doubles per warp: DE table, high columns, x0 hi/lo, row exponents (as
-    // doubles), rounded up to 32 bytes: the unit evaluator reads the DE table
-    // with 16-byte vector loads, so every warp's slice must start aligned.
-    static constexpr int SMEM_DOUBLES = (TERMS * N * C + NTP * N * C + 2 * N * C + N + 3) / 4 * 4;
+    // Unit-base lo words: registers, except complex n >= 21, where hi and lo
+    // of both parts (4n doubles) would spill; there they sit in a lane-private
+    // slot of the warp's shared slice.  (With 32 terms per unit the slot's
+    // per-unit traffic costs more than it saves wherever registers suffice.)
+    static constexpr bool LO_SMEM = C == 2 && N >= 21;
+    static constexpr int LO_DOUBLES = LO_SMEM ? 32 * N * C : 0;
+    // doubles per warp: DE table, high columns, x0 hi/lo, lo words, row
+    // exponents (as doubles), rounded up to 32 bytes: the unit evaluator reads
+    // the DE table with 16-byte vector loads, so every warp's slice must start
+    // aligned.
+    static constexpr int SMEM_DOUBLES = (TERMS * N * C + NTP * N * C + 2 * N * C + LO_DOUBLES + N + 3) / 4 * 4;
     static_assert(SMEM_DOUBLES % 4 == 0, "per-warp shared slice must keep 32-byte alignment");
 };
 
@@ -51,7 +58,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
     double* s_mt = s_de + TERMS * N * C;                  // [C][NTOP][N]
     double* s_x0h = s_mt + NTP * N * C;                   // [C][N]
     double* s_x0l = s_x0h + N * C;                        // [C][N]
-    int* s_exp = reinterpret_cast<int*>(s_x0l + N * C);   // [N]
+    double* s_lo = s_x0l + N * C;                         // [C][N][32] lane-private lo words (LO_SMEM)
+    int* s_exp = reinterpret_cast<int*>(s_lo + Q::LO_DOUBLES);  // [N]
 
     const int total_warps = gridDim.x * kWarpsPerCta;
     for (int m = blockIdx.x * kWarpsPerCta + wid; m < count; m += total_warps) {
@@ -99,7 +107,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
 #pragma unroll
         for (int c = 0; c < C; ++c) tot[c] = {0.0, 0.0};
         if (u0 < u1) {
-            double xh[C][N], xl[C][N];
+            // unit base: hi words in registers; lo words in registers or in the
+            // lane's shared slot (element (c, r) at [(c * N + r) * 32 + lane])
+            double xh[C][N];
+            double xlr[Q::LO_SMEM ? 1 : C * N];
+            double* xl = Q::LO_SMEM ? s_lo + lane : xlr;
+            constexpr int LS = Q::LO_SMEM ? 32 : 1;  // stride between elements
             const unsigned long long g0 = gray_of(u0);
 #pragma unroll
             for (int c = 0; c < C; ++c)
@@ -109,7 +122,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
                     for (int j = 0; j < NTOP; ++j)
                         if ((g0 >> j) & 1ull) x = dd_add_d(x, s_mt[c * NTP * N + j * N + r]);
                     xh[c][r] = x.hi;
-                    xl[c][r] = x.lo;
+                    xl[(c * N + r) * LS] = x.lo;
                 }
             unsigned long long u = u0;
             while (true) {
@@ -132,9 +145,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
                     for (int r = 0; r < N; ++r) {
                         const double v = s_mt[c * NTP * N + j * N + r];
                         dd s = two_sum(xh[c][r], add ? v : -v);
-                        dd z = fast_two_sum(s.hi, add_rn(s.lo, xl[c][r]));
+                        dd z = fast_two_sum(s.hi, add_rn(s.lo, xl[(c * N + r) * LS]));
                         xh[c][r] = z.hi;
-                        xl[c][r] = z.lo;
+                        xl[(c * N + r) * LS] = z.lo;
                     }
             }
         }

@@ -52,7 +52,7 @@ def test_batch_real_matches_single(spb, n):
         assert abs(got[k] - want) <= 1e-13 * max(abs(want), 1e-300) or abs(got[k] - want) <= 1e-14 * scale
 
 
-@pytest.mark.parametrize("n", [1, 2, 5, 11, 16, 20, 24])
+@pytest.mark.parametrize("n", [1, 2, 5, 11, 16, 20, 21, 23, 24])
 def test_batch_complex(spb, oracle, n):
     count = 6
     mats = np.stack([W.haar_block(n, seed=500 + k, N=64) for k in range(count)])
