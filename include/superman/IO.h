@@ -1,7 +1,10 @@
 // Matrix files, orderings, scaling and run settings — the reference's IO
-// class (IO/IO.h): readMatrix (:403-515), readComplex (:517-596), colSort /
-// rowSort (:677-833), scale (:109-161) and readSettings (:163-401), with the
-// same file format and error messages.
+// class (IO/IO.h): readMatrix (:403-515), readComplex (:517-596), the row
+// and column orderings colSort / rowSort (:677-833), skipOrder (:598-679),
+// colIndexMinimizationOrder (:891-924), UTOrder (:926-1002), alphaOrder
+// (:1004-1071), randomOrder (:1073-1093) with applyPermutations
+// (:1095-1112), scale (:109-161) and readSettings (:163-401), with the same
+// file format and error messages.
 //
 // File format: optional '%' comment lines, a header "rows cols lines", then
 // one "i j [value]" line per entry ("i j re im" for complex).  Indices are
@@ -14,9 +17,11 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <complex>
 #include <fstream>
 #include <iostream>
+#include <random>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -119,6 +124,119 @@ public:
 
     template <class S>
     static void rowSort(Matrix<S>* m, bool ascending = true) { permuteByDegree(m, ascending, false); }
+
+    // Moves row i to position rowTo[i] and column j to colTo[j] (IO/IO.h:1095-1112).
+    template <class S>
+    static void applyPermutations(Matrix<S>* m, const int* rowTo, const int* colTo)
+    {
+        const int n = m->nov;
+        S* nm = new S[(size_t)n * n];
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) nm[(size_t)rowTo[i] * n + colTo[j]] = m->mat[(size_t)i * n + j];
+        delete[] m->mat;
+        m->mat = nm;
+    }
+
+    // Upper-triangular-leaning order for the register-efficient generated
+    // kernels (IO/IO.h:926-1002): repeatedly take the column with the fewest
+    // nonzeros in rows not yet placed, place it next, then place (in index
+    // order) its rows not yet placed; rows never reached go last.
+    template <class S>
+    static void UTOrder(Matrix<S>* m)
+    {
+        const int n = m->nov;
+        std::vector<int> rowTo(n), colTo(n);
+        std::vector<long> open(n, 0);  // nonzeros of column j in unplaced rows; -1 once placed
+        for (int j = 0; j < n; ++j) open[j] = getColNNZ(m, j);
+        std::vector<char> placed(n, 0);
+        int nextRow = 0;
+        for (int step = 0; step < n; ++step) {
+            int c = -1;
+            for (int j = 0; j < n; ++j)
+                if (open[j] >= 0 && (c < 0 || open[j] < open[c])) c = j;
+            colTo[c] = step;
+            open[c] = -1;
+            for (int i = 0; i < n; ++i) {
+                if (m->mat[(size_t)i * n + c] == S(0) || placed[i]) continue;
+                placed[i] = 1;
+                rowTo[i] = nextRow++;
+                for (int j = 0; j < n; ++j)
+                    if (open[j] >= 0 && m->mat[(size_t)i * n + j] != S(0)) --open[j];
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            if (!placed[i]) rowTo[i] = nextRow++;
+        applyPermutations(m, rowTo.data(), colTo.data());
+    }
+
+    // The reference's earlier form of the same order (IO/IO.h:598-679): the
+    // same column choice and row placement, so the same result (rows never
+    // reached, possible only with an empty row, go last here as in UTOrder).
+    template <class S>
+    static void skipOrder(Matrix<S>* m)
+    {
+        UTOrder(m);
+    }
+
+    // Renumbers the columns by first appearance, scanning rows in order
+    // (IO/IO.h:891-924), so each row's columns lie as low as possible.
+    template <class S>
+    static void colIndexMinimizationOrder(Matrix<S>* m)
+    {
+        const int n = m->nov;
+        std::vector<int> rowTo(n), colTo(n, -1);
+        int next = 0;
+        for (int i = 0; i < n; ++i) {
+            rowTo[i] = i;
+            for (int j = 0; j < n; ++j)
+                if (m->mat[(size_t)i * n + j] != S(0) && colTo[j] < 0) colTo[j] = next++;
+        }
+        for (int j = 0; j < n; ++j)
+            if (colTo[j] < 0) colTo[j] = next++;  // empty columns keep a place
+        applyPermutations(m, rowTo.data(), colTo.data());
+    }
+
+    // Interleaves rows by degree (IO/IO.h:1004-1071): rows sorted by nonzero
+    // count (descending unless `ascending`), then one row from the first
+    // ceil(n/alpha) followed by alpha-1 from the end, repeatedly.  The
+    // reference gives every row left over after the interleave the same
+    // position (its final loop does not advance), which is not a
+    // permutation; here they take the following positions.
+    template <class S>
+    static void alphaOrder(Matrix<S>* m, unsigned alpha, bool ascending = false)
+    {
+        const int n = m->nov;
+        if (alpha < 1) alpha = 1;
+        std::vector<int> order(n), deg(n), rowTo(n), colTo(n);
+        for (int i = 0; i < n; ++i) {
+            order[i] = i;
+            deg[i] = getRowNNZ(m, i);
+            colTo[i] = i;
+        }
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return ascending ? deg[x] < deg[y] : deg[x] > deg[y]; });
+        const int split = (int)std::ceil((double)n / alpha) - 1;
+        int front = split, back = n - 1, cur = 0;
+        while (split < back) {
+            rowTo[order[front--]] = cur++;
+            for (unsigned k = 0; k + 1 < alpha && split < back; ++k) rowTo[order[back--]] = cur++;
+        }
+        while (front >= 0) rowTo[order[front--]] = cur++;
+        applyPermutations(m, rowTo.data(), colTo.data());
+    }
+
+    // Random row order (IO/IO.h:1073-1093); a fixed seed gives a repeatable
+    // order, seed 0 a random one as in the reference.
+    template <class S>
+    static void randomOrder(Matrix<S>* m, unsigned long long seed = 0)
+    {
+        const int n = m->nov;
+        std::vector<int> rowTo(n), colTo(n);
+        for (int i = 0; i < n; ++i) rowTo[i] = colTo[i] = i;
+        std::mt19937_64 g(seed ? seed : std::random_device{}());
+        std::shuffle(rowTo.begin(), rowTo.end(), g);
+        applyPermutations(m, rowTo.data(), colTo.data());
+    }
 
     // Sinkhorn-style alternating row/column scaling towards line sums
     // settings.scaleInto, settings.scalingIterationNo rounds; the factors are

@@ -252,6 +252,13 @@ SPB_API int spb_read_matrix(const char* path, int binary, int undirected, int is
  * all zeros).  Replaces dm() (IO/dm.cpp:441-501).  CPU only. */
 SPB_API int spb_dm_prune(const double* a, int n, double* out, int* has_perfect_matching);
 
+/* The reference's row/column orderings (IO/IO.h:598-1112) applied to a
+ * row-major n x n matrix: order is "colSort", "rowSort" (param 0 ascending,
+ * else descending), "skipOrder", "UTOrder", "colIndexMinimizationOrder",
+ * "alphaOrder" (param = alpha, 0 means 2) or "randomOrder" (param = seed,
+ * 0 random).  The permanent is unchanged.  CPU only. */
+SPB_API int spb_reorder(const double* a, int n, const char* order, unsigned long long param, double* out);
+
 /* The pieces DecomposePerman (CommonFiles/DecomposePerman.h:120-198) would
  * compute for a matrix, without computing them: *count pieces, sizes[k] and
  * their row-major entries concatenated in data.  Pass sizes = data = NULL to

@@ -149,6 +149,7 @@ SIGNATURES = {
                                      ctypes.POINTER(spb_pipeline_result)]),
     "spb_read_matrix": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP,
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP]),
+    "spb_reorder": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.c_char_p, ctypes.c_ulonglong, _DP]),
     "spb_dm_prune": (ctypes.c_int, [_DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int)]),
     "spb_decompose": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), _DP, ctypes.c_int, ctypes.c_size_t]),

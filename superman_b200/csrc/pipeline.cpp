@@ -216,3 +216,26 @@ extern "C" int spb_decompose(const double* a, int n, int* count, int* sizes, dou
         return st;
     });
 }
+
+extern "C" int spb_reorder(const double* a, int n, const char* order, unsigned long long param, double* out)
+{
+    if (!a || !out || !order || n < 0) {
+        spb_set_error("spb_reorder: null argument or negative n");
+        return SPB_ERR_INVALID;
+    }
+    return guarded([&] {
+        Matrix<double> m(n);
+        std::copy(a, a + (size_t)n * n, m.mat);
+        const std::string o(order);
+        if (o == "colSort") IO::colSort(&m, param == 0);
+        else if (o == "rowSort") IO::rowSort(&m, param == 0);
+        else if (o == "skipOrder") IO::skipOrder(&m);
+        else if (o == "UTOrder") IO::UTOrder(&m);
+        else if (o == "colIndexMinimizationOrder") IO::colIndexMinimizationOrder(&m);
+        else if (o == "alphaOrder") IO::alphaOrder(&m, (unsigned)(param ? param : 2));
+        else if (o == "randomOrder") IO::randomOrder(&m, param);
+        else throw std::runtime_error("spb_reorder: unknown order " + o);
+        std::copy(m.mat, m.mat + (size_t)n * n, out);
+        return (int)SPB_OK;
+    });
+}

@@ -173,3 +173,59 @@ def test_decompose_small_is_one_piece():
     a = W.dense_uniform(12, 1)
     pieces = decompose(a)
     assert len(pieces) == 1 and np.array_equal(pieces[0], a)
+
+
+# ---------------------------------------------------------------- orderings --
+def reorder(a, order, param=0):
+    L = _lib.lib()
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = np.zeros_like(a)
+    st = L.spb_reorder(a.ctypes.data_as(DP), a.shape[0], order.encode(), param, out.ctypes.data_as(DP))
+    assert st == 0, _lib.last_error()
+    return out
+
+
+def _is_permuted_copy(a, b):
+    """b equals a with rows and columns permuted (row and column multisets)."""
+    ra = sorted(tuple(sorted(r)) for r in a)
+    rb = sorted(tuple(sorted(r)) for r in b)
+    ca = sorted(tuple(sorted(c)) for c in a.T)
+    cb = sorted(tuple(sorted(c)) for c in b.T)
+    return ra == rb and ca == cb and np.isclose(a.sum(), b.sum())
+
+
+@pytest.mark.parametrize("order,param", [("colSort", 0), ("colSort", 1), ("rowSort", 0), ("rowSort", 1),
+                                         ("skipOrder", 0), ("UTOrder", 0), ("colIndexMinimizationOrder", 0),
+                                         ("alphaOrder", 2), ("alphaOrder", 3), ("randomOrder", 42)])
+def test_orderings_keep_permanent(oracle, order, param):
+    a = W.sparse_perm_plus(9, 3, extra=2)
+    b = reorder(a, order, param)
+    assert _is_permuted_copy(a, b)
+    assert oracle.exact_perm(b) == oracle.exact_perm(a)
+
+
+def test_utorder_triangularises():
+    """A row/column-shuffled upper-triangular pattern comes back upper
+    triangular."""
+    rng = np.random.default_rng(4)
+    t = np.triu(rng.random((10, 10)) + 0.5)
+    p, q = rng.permutation(10), rng.permutation(10)
+    b = reorder(t[p][:, q], "UTOrder")
+    assert _is_permuted_copy(t, b)
+    # the column with one nonzero comes first with its row, which covers every
+    # column; then the next, and so on: the result is upper triangular again
+    assert np.count_nonzero(np.tril(b != 0, -1)) == 0
+
+
+def test_alpha_order_is_a_permutation():
+    """Unlike the reference's final loop, every row keeps a distinct place."""
+    a = W.sparse_perm_plus(13, 8, extra=3)
+    for alpha in (2, 3, 4, 5):
+        assert _is_permuted_copy(a, reorder(a, "alphaOrder", alpha))
+
+
+def test_random_order_repeatable():
+    a = W.sparse_perm_plus(8, 2)
+    assert np.array_equal(reorder(a, "randomOrder", 7), reorder(a, "randomOrder", 7))
+    with pytest.raises(AssertionError):
+        reorder(a, "noSuchOrder")
