@@ -39,7 +39,7 @@ struct Problem {
     unsigned long long* list_u;    // [list_cap] unit index
     double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
     unsigned short* tmax;          // [grid*threads] highest bound bin of each thread's units
-    // Mode 1 direct listing: bound_pass counts the units per bound bin
+    // Mode 1 direct listing: bound_walk counts the units per bound bin
     // (pre_cnt), pick_list_bin sets *list_bin to the lowest bin whose tail fits
     // raw_cap, and the walk appends every unit at or above it (raw_*).
     unsigned* pre_cnt;             // [kHistBins]
@@ -51,7 +51,7 @@ struct Problem {
 };
 
 // Capacity of the mode-1 list (units); pick_list_bin aims at half of it so
-// that bins computed by the walk and by bound_pass may differ at bin edges.
+// that bins computed by the walk and by bound_walk may differ at bin edges.
 constexpr unsigned long long kRawCap = 1ull << 17;
 
 // Appends unit u (bound bin b) to the mode-1 list when b >= lbin.
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
 // pb.result, one warp per unit.  Defined in dense_refine.cu.
 int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s);
 
-// Mode-1 listing support (dense_refine.cu): bound_pass + pick_list_bin run
+// Mode-1 listing support (dense_refine.cu): bound_walk + pick_list_bin run
 // before the walk; collect then keeps the listed units whose bin >=
 // pb.thr_bin (pb.list_u, count in *pb.list_n), and the refine kernel
 // rebuilds each unit base from scratch (pb.list_x == nullptr).
