@@ -28,11 +28,15 @@ static double log2_perm_bound(const uint8_t* a, int n)
     return std::fmin(side(true), side(false));
 }
 
-static int pick_limbs(double bits)
+// Limbs for the NW sum Sigma = 2^(n-1) perm: |Sigma| < 2^(32L-1).
+static int pick_limbs(double perm_bits, int n)
 {
-    if (bits + 2 <= 128) return 4;
-    if (bits + 2 <= 192) return 6;
-    return 10;
+    const double bits = perm_bits + (n - 1) + 2;
+    if (bits <= 128) return 4;
+    if (bits <= 160) return 5;
+    if (bits <= 192) return 6;
+    if (bits <= 320) return 10;
+    return 12;
 }
 
 static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* limbs_out,
@@ -44,17 +48,19 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
         return SPB_ERR_INVALID;
     }
     std::memset(out, 0, sizeof(*out));
-    std::memset(limbs_out, 0, sizeof(uint32_t) * kMaxLimbs);
+    std::memset(limbs_out, 0, sizeof(uint32_t) * 10);
     spb_options opt;
     if (opt_in) opt = *opt_in; else spb_default_options(&opt);
     if (!a || n < 1 || n > kMaxN) {
         spb_set_error("binary permanent needs a non-null matrix and 1 <= n <= %d (got n=%d)", kMaxN, n);
         return out->status = SPB_ERR_INVALID;
     }
-    out->gray_steps = (uint64_t)n << n;
-    if (n == 1) {  // no subset walk needed
-        limbs_out[0] = a[0] ? 1u : 0u;
-        out->value = a[0] ? 1.0 : 0.0;
+    out->gray_steps = (uint64_t)n << (n - 1);
+    if (n <= 2) {  // fewer than two walk columns: direct
+        const unsigned v = n == 1 ? (a[0] ? 1u : 0u)
+                                  : (unsigned)((a[0] && a[3]) ? 1 : 0) + ((a[1] && a[2]) ? 1 : 0);
+        limbs_out[0] = v;
+        out->value = (double)v;
         out->elapsed_s = wall_seconds() - t_start;
         return out->status = SPB_OK;
     }
@@ -68,18 +74,19 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     Problem pb{};
     pb.n = n;
     const double bits = log2_perm_bound(a, n);
-    pb.limbs = pick_limbs(bits < 0 ? 0.0 : bits);
+    pb.limbs = pick_limbs(bits < 0 ? 0.0 : bits, n);
+    // the NW walk runs over the n-1 columns other than the last
     int w = opt.unit_bits > 0 ? opt.unit_bits : 8;
     if (opt.unit_bits <= 0)
-        while (w > 2 && (((size_t)1 << w) * n * 4 > 32 * 1024 || n - w < 16)) --w;
+        while (w > 2 && (((size_t)1 << w) * n * 4 > 32 * 1024 || n - 1 - w < 16)) --w;
     if (w > 12) w = 12;
-    if (w > n) w = n;
+    if (w > n - 1) w = n - 1;
     if (w < 2) w = 2;
     pb.w = w;
-    pb.units = 1ull << (n - w);
-    const int terms = 1 << w, ntop = n - w;
+    pb.units = 1ull << (n - 1 - w);
+    const int terms = 1 << w, ntop = n - 1 - w;
 
-    const int tmax = bin_max_threads(n);
+    const int tmax = bin_max_threads(n, pb.limbs);
     int threads = opt.threads_per_block > 0 ? (opt.threads_per_block / 32) * 32 : tmax;
     if (threads > tmax) threads = tmax;
     if (threads < 32) threads = 32;
@@ -90,17 +97,24 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     pb.grid = blocks;
     const size_t smem = sizeof(int) * terms * n + align_up((size_t)(ntop > 0 ? ntop : 1) * n, 16);
 
-    // host-built tables
+    // host-built tables: x'_r = 2 a_{r,n-1} - rowsum_r, doubled low-column
+    // counts, doubled high columns
+    std::vector<int> x0(n);
+    for (int r = 0; r < n; ++r) {
+        int rs = 0;
+        for (int j = 0; j < n; ++j) rs += a[r * n + j] ? 1 : 0;
+        x0[r] = 2 * (a[r * n + n - 1] ? 1 : 0) - rs;
+    }
     std::vector<int> dei((size_t)terms * n);
     for (int d = 0; d < terms; ++d)
         for (int r = 0; r < n; ++r) {
             int c = 0;
-            for (int j = 0; j < w; ++j) c += ((d >> j) & 1) && a[r * n + j] ? 1 : 0;
+            for (int j = 0; j < w; ++j) c += ((d >> j) & 1) && a[r * n + j] ? 2 : 0;
             dei[((size_t)(d / 4) * n + r) * 4 + (d % 4)] = c;
         }
     std::vector<int8_t> mt((size_t)(ntop > 0 ? ntop : 1) * n, 0);
     for (int j = 0; j < ntop; ++j)
-        for (int r = 0; r < n; ++r) mt[(size_t)j * n + r] = a[r * n + w + j] ? 1 : 0;
+        for (int r = 0; r < n; ++r) mt[(size_t)j * n + r] = a[r * n + w + j] ? 2 : 0;
 
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -108,6 +122,7 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
         off = align_up(off + bytes, 256);
         return o;
     };
+    const size_t o_x0 = take(sizeof(int) * n);
     const size_t o_de = take(sizeof(int) * dei.size());
     const size_t o_mt = take(mt.size());
     const size_t o_part = take(sizeof(uint32_t) * kMaxLimbs * blocks);
@@ -115,6 +130,7 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     const size_t o_res = take(sizeof(uint32_t) * kMaxLimbs);
     if ((st = ensure_scratch(ctx, off)) != SPB_OK) return out->status = st;
     char* base = static_cast<char*>(ctx->scratch);
+    pb.x0 = reinterpret_cast<const int*>(base + o_x0);
     pb.dei = reinterpret_cast<const int*>(base + o_de);
     pb.mt = reinterpret_cast<const int8_t*>(base + o_mt);
     pb.partials = reinterpret_cast<uint32_t*>(base + o_part);
@@ -122,6 +138,7 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     pb.result = reinterpret_cast<uint32_t*>(base + o_res);
 
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
+    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_x0, x0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
     SPB_CUDA_TRY(cudaMemcpyAsync(base + o_de, dei.data(), sizeof(int) * dei.size(), cudaMemcpyHostToDevice, stream));
     SPB_CUDA_TRY(cudaMemcpyAsync(base + o_mt, mt.data(), mt.size(), cudaMemcpyHostToDevice, stream));
     SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
@@ -137,7 +154,7 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));
 
     const int L = pb.limbs;
-    if (n & 1) {  // perm = (-1)^n * sum, negate mod 2^(32L)
+    if (!(n & 1)) {  // perm = (+-) Sigma / 2^(n-1), + for odd n: negate mod 2^(32L)
         uint64_t c = 1;
         for (int l = 0; l < L; ++l) {
             uint64_t t = (uint64_t)(~res[l]) + c;
@@ -145,21 +162,32 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
             c = t >> 32;
         }
     }
+    // arithmetic shift right by n-1 bits (Sigma is a multiple of 2^(n-1))
     const bool neg = (res[L - 1] >> 31) & 1u;
-    for (int l = 0; l < kMaxLimbs; ++l) limbs_out[l] = l < L ? res[l] : (neg ? 0xffffffffu : 0u);
+    uint32_t ext[kMaxLimbs + 2];
+    for (int l = 0; l < kMaxLimbs + 2; ++l) ext[l] = l < L ? res[l] : (neg ? 0xffffffffu : 0u);
+    const int sh = n - 1, ws = sh / 32, bs = sh % 32;
+    uint32_t shifted[kMaxLimbs];
+    for (int l = 0; l < kMaxLimbs; ++l) {
+        const uint32_t lo = l + ws < kMaxLimbs + 2 ? ext[l + ws] : (neg ? 0xffffffffu : 0u);
+        const uint32_t hi = l + ws + 1 < kMaxLimbs + 2 ? ext[l + ws + 1] : (neg ? 0xffffffffu : 0u);
+        shifted[l] = bs ? (lo >> bs) | (hi << (32 - bs)) : lo;
+    }
+    constexpr int kOutLimbs = 10;  // the C ABI's 320-bit result
+    for (int l = 0; l < kOutLimbs; ++l) limbs_out[l] = shifted[l];
     // double approximation of the signed integer
     double v = 0.0;
-    uint32_t mag[kMaxLimbs];
+    uint32_t mag[kOutLimbs];
     std::memcpy(mag, limbs_out, sizeof(mag));
     if (neg) {
         uint64_t c = 1;
-        for (int l = 0; l < kMaxLimbs; ++l) {
+        for (int l = 0; l < kOutLimbs; ++l) {
             uint64_t t = (uint64_t)(~mag[l]) + c;
             mag[l] = (uint32_t)t;
             c = t >> 32;
         }
     }
-    for (int l = kMaxLimbs - 1; l >= 0; --l) v = v * 4294967296.0 + (double)mag[l];
+    for (int l = kOutLimbs - 1; l >= 0; --l) v = v * 4294967296.0 + (double)mag[l];
     out->value = neg ? -v : v;
     out->kernel_s = ms * 1e-3;
     out->device_s = ms_call * 1e-3;

@@ -1,20 +1,26 @@
-// Exact 0/1 permanent: plain Ryser over all 2^n column subsets,
-//   perm(A) = (-1)^n sum_S (-1)^|S| prod_r x_r(S),   x_r(S) = sum_{j in S} a_rj,
-// in wrap-around integer arithmetic modulo 2^(32L).  The host picks L from a
-// Bregman-Minc bound so that |perm| < 2^(32L-1): the result is then exact.
+// Exact 0/1 permanent by the Nijenhuis–Wilf form of Ryser's formula in
+// integers.  With x'_r(S) = 2 a_{r,n-1} - rowsum_r + 2 sum_{j in S} a_rj
+// (twice the NW row value, an integer in [-n, n]) over the subsets S of
+// columns 0..n-2,
+//   Sigma = sum_S (-1)^|S| prod_r x'_r(S) = 2^(n-1) * (+-) perm(A)
+// (+ for odd n, - for even), computed in wrap-around integer arithmetic
+// modulo 2^(32L).  The host picks L from a Bregman-Minc bound so that
+// |Sigma| < 2^(32L-1), then shifts Sigma right by n-1 bits: the result is
+// exact.  Half the subsets of plain Ryser, for n - 1 more accumulator bits.
 //
 // The reference has no integer path: 0/1 input goes through its FP64 NW
 // walk (IO/IO.h:441-443 feeding Algorithms/GPU/Dense/dpSingleGPU.cuh), whose
 // result is off by ~1e-10 relative at n=30.
 //
 // Layout mirrors the dense walk: the w low columns are enumerated from a
-// shared table DEI[d][r] = number of ones of row r among the columns of d
-// (grouped [d/4][r][d%4], so one 16-byte broadcast load serves four terms);
-// the n-w high columns form a unit index walked in Gray order per thread with
-// the integer unit base xtop_r in registers.  Each term multiplies up to K
-// row sums in 32 bits (n^K < 2^32), then folds those partial products into L
-// 32-bit limbs with 32x32->64 multiply-adds.  Unit sums and the grid
-// reduction are exact, so the result does not depend on the launch shape.
+// shared table DEI[d][r] = twice the number of ones of row r among the
+// columns of d (grouped [d/4][r][d%4], so one 16-byte broadcast load serves
+// four terms); the n-1-w high columns form a unit index walked in Gray order
+// per thread with the integer unit base xtop_r in registers.  Each term
+// multiplies up to K row values in signed 32-bit arithmetic (n^K < 2^31, so
+// exact), folds the magnitudes into L 32-bit limbs with 32x32->64
+// multiply-adds and applies the sign once.  Unit sums and the grid reduction
+// are exact, so the result does not depend on the launch shape.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,28 +32,45 @@ namespace spb {
 namespace binary {
 
 constexpr int kMaxN = 63;
-constexpr int kMaxLimbs = 10;
+constexpr int kMaxLimbs = 12;   // accumulator limbs (the result needs at most 10)
 
 struct Problem {
     int n, w, limbs, grid;
-    unsigned long long units;  // 2^(n-w) Gray units of 2^w terms each
-    const int* dei;            // [2^w/4][n][4] low-column row counts
-    const int8_t* mt;          // [n-w][n] high columns (0/1)
+    unsigned long long units;  // 2^(n-1-w) Gray units of 2^w terms each
+    const int* x0;             // [n] 2 a_{r,n-1} - rowsum_r
+    const int* dei;            // [2^w/4][n][4] twice the low-column row counts
+    const int8_t* mt;          // [n-1-w][n] high columns, doubled (0/2)
     uint32_t* partials;        // [grid][limbs]
     unsigned* ticket;          // last-CTA election (reset by the kernel)
     uint32_t* result;          // [limbs] sum over subsets, mod 2^(32*limbs)
 };
 
-// Rows per 32-bit partial product: largest K with N^K < 2^32.
+// Rows per signed 32-bit partial product: largest K with N^K < 2^31
+// (|x'_r| <= N, so the product is exact).
 __host__ __device__ constexpr int rows_per_word(int n)
 {
     int k = 1;
-    unsigned long long p = (unsigned long long)(n > 1 ? n : 2);
-    while (p * (unsigned long long)(n > 1 ? n : 2) < (1ull << 32) && k < 16) {
-        p *= (unsigned long long)(n > 1 ? n : 2);
+    const unsigned long long b = (unsigned long long)(n > 1 ? n : 2);
+    unsigned long long p = b;
+    while (p * b < (1ull << 31) && k < 16) {
+        p *= b;
         ++k;
     }
     return k;
+}
+
+// a += p, or a -= p when sub, modulo 2^(32L): a + (p xor mask) + sub.
+template <int L>
+__device__ __forceinline__ void limb_add_signed(uint32_t (&a)[L], const uint32_t (&p)[L], bool sub)
+{
+    const uint32_t mask = sub ? 0xffffffffu : 0u;
+    uint64_t c = sub ? 1u : 0u;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        uint64_t t = (uint64_t)a[i] + (p[i] ^ mask) + c;
+        a[i] = (uint32_t)t;
+        c = t >> 32;
+    }
 }
 
 template <int L>
@@ -74,23 +97,26 @@ __device__ __forceinline__ void limb_sub(uint32_t (&a)[L], const uint32_t (&b)[L
     }
 }
 
-// prod_r x_r mod 2^(32L) for one term; x_r = xt[r] + de(r).
+// prod_r x'_r mod 2^(32L) for one term; x'_r = xt[r] + de(r), signed.
 template <int N, int L, int G>
-__device__ __forceinline__ void term_product(const int (&xt)[N], const int* __restrict__ de, int i,
+__device__ __forceinline__ bool term_product(const int (&xt)[N], const int* __restrict__ de, int i,
                                              uint32_t (&p)[L])
 {
     constexpr int K = rows_per_word(N);
     constexpr int NG = (N + K - 1) / K;
 #pragma unroll
     for (int l = 0; l < L; ++l) p[l] = 0u;
+    bool neg = false;
 #pragma unroll
     for (int g = 0; g < NG; ++g) {
-        uint32_t w = 1u;
+        int sw = 1;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int r = g * K + k;
-            if (r < N) w *= (uint32_t)(xt[r] + de[r * G + i]);
+            if (r < N) sw *= xt[r] + de[r * G + i];
         }
+        neg ^= sw < 0;
+        const uint32_t w = (uint32_t)(sw < 0 ? -sw : sw);
         if (g == 0) {
             p[0] = w;
         } else {
@@ -106,6 +132,7 @@ __device__ __forceinline__ void term_product(const int (&xt)[N], const int* __re
             }
         }
     }
+    return neg;  // the term is -p when set
 }
 
 // Sum over one unit: sum_d (-1)^popc(d) prod_r (xt_r + DEI[d][r]).
@@ -119,21 +146,18 @@ __device__ __forceinline__ void unit_sum_bin(const int (&xt)[N], const int* __re
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const int* de = s_de + q * (N * G);
-        uint32_t p0[L], p1[L], p2[L], p3[L];
-        term_product<N, L, G>(xt, de, 0, p0);
-        term_product<N, L, G>(xt, de, 1, p1);
-        term_product<N, L, G>(xt, de, 2, p2);
-        term_product<N, L, G>(xt, de, 3, p3);
-        // group signs relative to popc(q): + - - +
-        limb_add<L>(p0, p3);
-        limb_add<L>(p1, p2);
-        if (__popc(q) & 1) {
-            limb_sub<L>(acc, p0);
-            limb_add<L>(acc, p1);
-        } else {
-            limb_add<L>(acc, p0);
-            limb_sub<L>(acc, p1);
-        }
+        // group signs relative to popc(q): + - - +; each term also carries
+        // the sign of its product
+        const bool odd = __popc(q) & 1;
+        uint32_t p[L];
+        bool neg = term_product<N, L, G>(xt, de, 0, p);
+        limb_add_signed<L>(acc, p, neg != odd);
+        neg = term_product<N, L, G>(xt, de, 1, p);
+        limb_add_signed<L>(acc, p, neg == odd);
+        neg = term_product<N, L, G>(xt, de, 2, p);
+        limb_add_signed<L>(acc, p, neg == odd);
+        neg = term_product<N, L, G>(xt, de, 3, p);
+        limb_add_signed<L>(acc, p, neg != odd);
     }
 }
 
@@ -146,16 +170,16 @@ __device__ __forceinline__ void shfl_add(uint32_t (&v)[L], int m)
     limb_add<L>(v, o);
 }
 
-// Threads per CTA: 512 keeps n <= 36 spill-free within 128 registers; larger
-// n (wider products, more limbs) gets 255 registers at 256 threads.
-__host__ __device__ constexpr int bin_max_threads(int n) { return n <= 36 ? 512 : 256; }
+// Threads per CTA: 512 (128 registers) keeps 4 limbs spill-free up to
+// n = 28; larger n or more limbs get 255 registers at 256 threads.
+__host__ __device__ constexpr int bin_max_threads(int n, int limbs) { return (limbs <= 4 && n <= 28) ? 512 : 256; }
 
 template <int N, int L>
-__global__ void __launch_bounds__(bin_max_threads(N), 1) walk_binary(Problem pb)
+__global__ void __launch_bounds__(bin_max_threads(N, L), 1) walk_binary(Problem pb)
 {
     constexpr int G = 4;
     extern __shared__ __align__(16) int smem_i[];
-    const int w = pb.w, terms = 1 << w, nq = terms / G, ntop = N - w;
+    const int w = pb.w, terms = 1 << w, nq = terms / G, ntop = N - 1 - w;
     const int tid = threadIdx.x, bd = blockDim.x;
     int* s_de = smem_i;
     int8_t* s_mt = reinterpret_cast<int8_t*>(s_de + terms * N);
@@ -174,7 +198,7 @@ __global__ void __launch_bounds__(bin_max_threads(N), 1) walk_binary(Problem pb)
         int xt[N];
         const unsigned long long g0 = gray_of(u0);
 #pragma unroll
-        for (int r = 0; r < N; ++r) xt[r] = 0;
+        for (int r = 0; r < N; ++r) xt[r] = pb.x0[r];
         for (int j = 0; j < ntop; ++j) {  // columns outermost, rows independent
             if (!((g0 >> j) & 1ull)) continue;
 #pragma unroll

@@ -1,11 +1,9 @@
-// walk_binary<N, L> instantiations (L=4).
+// walk_binary<N, L> instantiations (L=4 n=3..33).
 #include "binary_launch.cuh"
 
 namespace spb {
 namespace binary {
 
-template int launch_bin_n<1, 4>(const Problem&, int, int, size_t, cudaStream_t);
-template int launch_bin_n<2, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<3, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<4, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<5, 4>(const Problem&, int, int, size_t, cudaStream_t);
@@ -35,6 +33,8 @@ template int launch_bin_n<28, 4>(const Problem&, int, int, size_t, cudaStream_t)
 template int launch_bin_n<29, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<30, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<31, 4>(const Problem&, int, int, size_t, cudaStream_t);
+template int launch_bin_n<32, 4>(const Problem&, int, int, size_t, cudaStream_t);
+template int launch_bin_n<33, 4>(const Problem&, int, int, size_t, cudaStream_t);
 
 }  // namespace binary
 }  // namespace spb

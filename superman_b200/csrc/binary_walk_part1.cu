@@ -1,11 +1,9 @@
-// walk_binary<N, L> instantiations (L=4).
+// walk_binary<N, L> instantiations (L=4 n=34..63).
 #include "binary_launch.cuh"
 
 namespace spb {
 namespace binary {
 
-template int launch_bin_n<32, 4>(const Problem&, int, int, size_t, cudaStream_t);
-template int launch_bin_n<33, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<34, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<35, 4>(const Problem&, int, int, size_t, cudaStream_t);
 template int launch_bin_n<36, 4>(const Problem&, int, int, size_t, cudaStream_t);
