@@ -1,7 +1,7 @@
 """Benchmark of the Ryser / Gray-code permanent hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dense32|dense24|complex28|binary36|sparse40]
+                    [--workload dense32|dense24|complex28|binary36|sparse40|batch20|approx100|serve|...]
 
 A step is one permanent of the workload matrix (the headline: dense real FP64
 n=32, entries U[0,1) from SplitMix64 seed 7).  The metric is Gray steps per
@@ -46,6 +46,8 @@ WORKLOADS = {
     "binary28": ("binary", 28, 4, "binary_bernoulli0.5_or_identity_n28_seed4"),
     "batch20": ("batch", 20, 11, "batch_4096_dense_u01_n20_seed11"),
     "sparse40": ("sparse", 40, 5, "sparse_perm_plus3_u0.5-1.5_n40_seed5"),
+    # sampling permanent (the reference's algorithm=approximation) beyond n=63
+    "approx100": ("approx", 100, 5, "sampling_pattern_perm_plus3_n100_seed5_4Msamples"),
 }
 
 # DRAM bytes (read + write) per walk_real<32> launch, from one ncu capture of
@@ -508,6 +510,25 @@ def other_arm(args, wl):
                 "clocks": clk.summary(), "gpu_launches": args.steps}
         print(json.dumps(line), flush=True)
         return 0
+    if kind == "approx":
+        a = (W.sparse_perm_plus(n, seed) != 0).astype(np.uint8)
+        samples = 1 << 22
+        for _ in range(args.warmup):
+            S.perm_approx(a, samples=1 << 16, seed=1)
+        with ClockSampler(0) as clk:
+            rs = [S.perm_approx(a, samples=samples, seed=1 + k) for k in range(args.steps)]
+        t = statistics.mean(x.kernel_s for x in rs)
+        dt = statistics.mean(x.time for x in rs)
+        line = {"metric": "samples_per_s", "value": samples / t, "unit": "samples/s",
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "n": n, "samples": samples, "estimate": rs[0].permanent,
+                           "rel_std_error": rs[0].err_est,
+                           "timing": "kernel events of spb_perm_approx; samples per step = 2^22"},
+                "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+        return 0
     if kind == "binary":
         a = W.binary_bernoulli(n, seed)
         _lib.check(L.spb_measure_pipe_peak(0, 1, ctypes.byref(peak)))
@@ -600,7 +621,7 @@ def main():
         return serve_arm(args, args.workload)
     if args.impl == "reference":
         return reference_arm(args, args.workload)
-    if WORKLOADS[args.workload][0] in ("binary", "sparse", "batch"):
+    if WORKLOADS[args.workload][0] in ("binary", "sparse", "batch", "approx"):
         return other_arm(args, args.workload)
     return ours_arm(args, args.workload)
 
