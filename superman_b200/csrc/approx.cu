@@ -182,7 +182,7 @@ struct Sums {
     double* per_sample;      // optional: estimates of samples [first, first + count)
 };
 
-__global__ void __launch_bounds__(128) rasmussen_kernel(Pattern P, Lane L0, unsigned long long first,
+__global__ void __launch_bounds__(128, 8) rasmussen_kernel(Pattern P, Lane L0, unsigned long long first,
                                                         unsigned long long count, unsigned long long seed, Sums S)
 {
     Lane L = L0;
@@ -309,10 +309,11 @@ int run(const int* cptrs, const int* rows, int n, unsigned long long first, unsi
     SPB_CUDA_TRY(cudaSetDevice(ctx->device));
     cudaStream_t stream = call_stream(ctx, &opt);
 
-    // Launch shape: 4 CTAs of 128 threads per SM, fewer when the per-thread
+    // Launch shape: 8 CTAs of 128 threads per SM (the sampler is latency-bound;
+    // 64 registers a thread let all of them be resident), fewer when the per-thread
     // state (5n words) would pass 2 GB or there are fewer samples.
     const int threads = 128;
-    unsigned long long T = (unsigned long long)ctx->sm_count * 4 * threads;
+    unsigned long long T = (unsigned long long)ctx->sm_count * 8 * threads;
     const unsigned long long cap = (2ull << 30) / (20ull * (unsigned long long)n);
     if (T > cap) T = cap;
     if (T > count) T = count;
