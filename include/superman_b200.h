@@ -323,6 +323,12 @@ SPB_API int spb_server_destroy(void* server);
 /* Steady-clock seconds on the clock the request timestamps use. */
 SPB_API double spb_now(void);
 
+/* Fault injection for tests: each of the next `count` library allocations
+ * (device scratch, refinement list, pinned staging, serving slots) fails with
+ * SPB_ERR_OOM without allocating; the calls after them work normally.  0
+ * clears it.  Host-side only: no GPU fault is involved. */
+SPB_API void spb_debug_fail_allocations(int count);
+
 /* Measured pipe throughput used as the roofline denominator: which = 0 gives
  * FP64 FMA thread-instructions per second, which = 1 gives int32 multiply-add
  * thread-instructions per second (best of three timed launches).  No

@@ -166,6 +166,7 @@ SIGNATURES = {
     "spb_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(spb_server_stats)]),
     "spb_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "spb_now": (ctypes.c_double, []),
+    "spb_debug_fail_allocations": (None, [ctypes.c_int]),
     "spb_measure_pipe_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_double)]),
 }

@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <memory>
 
 #include "spb_common.cuh"
@@ -106,8 +107,24 @@ DeviceContext* get_context(int device, int* st)
     return g_ctx[device].get();
 }
 
+// Allocation failures injected by spb_debug_fail_allocations: each of the
+// next g_fail_allocs calls of ensure_scratch / ensure_list / ensure_pinned
+// reports SPB_ERR_OOM without allocating (or freeing) anything.
+static std::atomic<int> g_fail_allocs{0};
+
+bool injected_failure(const char* what)
+{
+    int k = g_fail_allocs.load();
+    while (k > 0 && !g_fail_allocs.compare_exchange_weak(k, k - 1)) {
+    }
+    if (k <= 0) return false;
+    spb_set_error("%s: allocation failure injected for testing", what);
+    return true;
+}
+
 int ensure_scratch(DeviceContext* ctx, size_t bytes)
 {
+    if (injected_failure("scratch")) return SPB_ERR_OOM;
     if (bytes <= ctx->scratch_bytes) return SPB_OK;
     if (ctx->scratch) {
         cudaStreamSynchronize(ctx->stream);
@@ -127,6 +144,7 @@ int ensure_scratch(DeviceContext* ctx, size_t bytes)
 
 int ensure_list(DeviceContext* ctx, size_t bytes)
 {
+    if (injected_failure("refinement list")) return SPB_ERR_OOM;
     if (bytes <= ctx->list_bytes) return SPB_OK;
     if (ctx->list) {
         cudaStreamSynchronize(ctx->stream);
@@ -146,6 +164,7 @@ int ensure_list(DeviceContext* ctx, size_t bytes)
 
 int ensure_pinned(DeviceContext* ctx, size_t bytes)
 {
+    if (injected_failure("pinned")) return SPB_ERR_OOM;
     if (bytes <= ctx->pinned_bytes) return SPB_OK;
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     ctx->pinned = nullptr;
@@ -161,3 +180,5 @@ int ensure_pinned(DeviceContext* ctx, size_t bytes)
 }
 
 }  // namespace spb
+
+extern "C" void spb_debug_fail_allocations(int count) { spb::g_fail_allocs.store(count > 0 ? count : 0); }

@@ -40,6 +40,10 @@ int ensure_list(DeviceContext* ctx, size_t bytes);
 // Ensures ctx->pinned holds at least `bytes` of page-locked host memory.
 int ensure_pinned(DeviceContext* ctx, size_t bytes);
 
+// True (and the error message set) when an allocation failure injected by
+// spb_debug_fail_allocations is due; every allocation site checks it first.
+bool injected_failure(const char* what);
+
 // Resolves the stream to use for a call.
 inline cudaStream_t call_stream(DeviceContext* ctx, const spb_options* opt)
 {

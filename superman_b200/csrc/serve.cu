@@ -125,7 +125,8 @@ int Server::start()
     const size_t out_doubles = (size_t)cfg.max_batch * 4;
     slots.resize(cfg.slots);
     for (auto& s : slots) {
-        if (cudaMalloc(&s.d_in, in_doubles * sizeof(double)) != cudaSuccess ||
+        if (injected_failure("serving slot") ||
+            cudaMalloc(&s.d_in, in_doubles * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&s.d_out, out_doubles * sizeof(double)) != cudaSuccess ||
             cudaMallocHost(&s.h_in, in_doubles * sizeof(double)) != cudaSuccess ||
             cudaMallocHost(&s.h_out, out_doubles * sizeof(double)) != cudaSuccess) {

@@ -82,7 +82,11 @@ struct Choice {
 // code flips high column j once every 2^(j+1) units.
 void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, bool dd, Choice* best)
 {
-    const int wmax = std::min(10, n - 1 - min_ntop);
+    // The low-column table obeys the dense walk's 64 KB budget (2^w n
+    // doubles), so the refinement kernel can hold it, hi and lo, in shared
+    // memory.
+    int wmax = std::min(10, n - 1 - min_ntop);
+    while (wmax > 2 && ((size_t)1 << wmax) * (size_t)n * sizeof(double) > (size_t)64 * 1024) --wmax;
     for (int last = 0; last < n; ++last) {
         std::vector<char> used(n, 0);
         used[last] = 1;

@@ -83,3 +83,14 @@ def test_plan_rejects_bad_arguments():
     L = _lib.lib()
     assert L.spb_sparse_plan(a.ctypes.data_as(DP), 0, 0, ctypes.byref(na), ctypes.byref(w), None, None) != 0
     assert L.spb_sparse_plan(a.ctypes.data_as(DP), 64, 0, ctypes.byref(na), ctypes.byref(w), None, None) != 0
+
+
+def test_plan_table_budget():
+    """A block-diagonal matrix invites many low columns (they touch few rows);
+    the plan keeps the low-column table within 64 KB (2^w * n doubles)."""
+    a = np.zeros((30, 30))
+    a[:14, :14] = W.dense_uniform(14, 13)
+    a[14:, 14:] = W.dense_uniform(16, 14)
+    na, w, ro, co = plan(a)
+    check_plan(a, na, w, ro, co)
+    assert (1 << w) * 30 * 8 <= 64 * 1024
