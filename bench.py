@@ -198,11 +198,70 @@ def run_cpu_baseline(kind, n, seed, steps=1):
                       f"thread_count={cores}); mean of {steps} run(s), {t:.3f} s each"}, times
 
 
+def unavailable_line(why):
+    print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+    return 0
+
+
+def reference_other(args, kind, n, seed, desc):
+    """Reference arm for the sparse-pipeline and 0/1 workloads: the reference's
+    CPU program on the same input (0/1: binary=true, its FP64 path), on all host
+    cores; the 0/1 size is bounded like the dense CPU sample."""
+    import numpy as np
+    from superman_b200 import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    if not os.path.exists(O.ref_binary_path()):
+        return unavailable_line("the reference CPU program (oracle/_ref) is not built")
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "m.mtx")
+        if kind == "sparse":
+            a = W.sparse_perm_plus(n, seed)
+            write_mtx(p, a)
+            extra, m = [], n
+        else:
+            m = cpu_sample("dense", n, seed, cores)
+            a = W.binary_bernoulli(m, seed)
+            with open(p, "w") as f:  # binary=true reads "i j" lines
+                ij = np.argwhere(a != 0)
+                f.write(f"{m} {m} {len(ij)}\n" + "".join(f"{i + 1} {j + 1}\n" for i, j in ij))
+            extra = ["binary=true"]
+        for _ in range(args.warmup):
+            O.run_reference(p, threads=cores, extra=extra, timeout=1800)
+        times = [O.run_reference(p, threads=cores, extra=extra, timeout=1800)[1] for _ in range(args.steps)]
+    t = statistics.mean(times)
+    if kind == "sparse":
+        metric, value, unit = "sparse_pipeline_perms_per_s", 1.0 / t, "perms/s"
+        sample = f"reference CPU program on the n={n} matrix (its decomposition and sparse Ryser)"
+    else:
+        metric, value, unit = "ryser_gray_steps_per_s", m * 2 ** (m - 1) / t, "gray-steps/s (NW, n*2^(n-1))"
+        sample = f"reference CPU program, binary=true, on the same generator at n={m}"
+    cb = {"value": value, "unit": unit, "cores": cores, "kind": "reference",
+          "sample": f"{sample}; mean of {args.steps} run(s), {t:.3f} s each"}
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "kind": kind, "n": n, "seed": seed}, "impl": "reference",
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def reference_arm(args, wl):
-    kind, n, seed, desc = WORKLOADS[wl]
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
+    if wl in SERVE_WORKLOADS:
+        return unavailable_line("the reference has no serving loop: it computes one matrix per process run")
+    kind, n, seed, desc = WORKLOADS[wl]
+    if kind == "batch":
+        return unavailable_line("the reference has no batched entry point: one matrix per process run")
+    if kind == "approx":
+        return unavailable_line("the reference's approximation (aspSingleGPU) exists only in its GPU build; "
+                                "this arm times the reference's CPU program, which has no approximation")
+    if kind in ("sparse", "binary"):
+        return reference_other(args, kind, n, seed, desc)
     for _ in range(args.warmup):
         run_cpu_baseline(kind, n, seed, steps=1)
     cb, times = run_cpu_baseline(kind, n, seed, steps=args.steps)
@@ -617,10 +676,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload in SERVE_WORKLOADS:
-        return serve_arm(args, args.workload)
     if args.impl == "reference":
         return reference_arm(args, args.workload)
+    if args.workload in SERVE_WORKLOADS:
+        return serve_arm(args, args.workload)
     if WORKLOADS[args.workload][0] in ("binary", "sparse", "batch", "approx"):
         return other_arm(args, args.workload)
     return ours_arm(args, args.workload)
