@@ -376,20 +376,45 @@ def ours_arm(args, wl):
                                "MEASURED_PEAKS.json has no FP64 figure",
                 "algorithmic_per_launch": alg}
 
-    err = None
     golden_name = {"dense32": "dense_u01_n32_s7", "dense24": "dense_u01_n24_s3",
                    "complex28": "complex_haar_n28_s6"}.get(wl)
     golden = os.path.join(ROOT, "tests", "golden", f"{golden_name}.json")
-    if golden_name and os.path.exists(golden) and rank == 0:
+
+    def err_vs_exact(v):
+        """Relative error of v against the committed exact value (None when
+        this workload has no fixture)."""
+        if not (golden_name and os.path.exists(golden)):
+            return None
         from fractions import Fraction
         g = json.load(open(golden))
-        if comps == 1 and [float(v).hex() for v in a.ravel()] == g["hex"]:
+        if comps == 1 and [float(x).hex() for x in a.ravel()] == g["hex"]:
             ex = Fraction(g["exact"])
-            err = float(abs(Fraction(value_dev) - ex) / abs(ex))
-        elif comps == 2 and [float(v.real).hex() for v in a.ravel()] == g["re_hex"]:
+            return float(abs(Fraction(v) - ex) / abs(ex))
+        if comps == 2 and [float(x.real).hex() for x in a.ravel()] == g["re_hex"]:
             er, ei = Fraction(g["exact_re"]), Fraction(g["exact_im"])
-            d2 = (Fraction(value_dev.real) - er) ** 2 + (Fraction(value_dev.imag) - ei) ** 2
-            err = math.sqrt(float(d2 / (er * er + ei * ei)))
+            d2 = (Fraction(v.real) - er) ** 2 + (Fraction(v.imag) - ei) ** 2
+            return math.sqrt(float(d2 / (er * er + ei * ei)))
+        return None
+
+    err = err_vs_exact(value_dev) if rank == 0 else None
+
+    # The FP32-product variant beside the complex line, with its measured error.
+    f32 = None
+    if comps == 2 and rank == 0 and n <= 40:
+        o32 = _lib.default_options(device=device, precision=_lib.SPB_PREC_FP32)
+        r32 = _lib.spb_result()
+        for _ in range(2):
+            _lib.check(fn_dev(ctypes.c_void_p(dev_a.data_ptr()), n, ctypes.byref(o32), ctypes.byref(r32)))
+        ks = []
+        for _ in range(5):
+            flush.zero_()
+            torch.cuda.synchronize()
+            _lib.check(fn_dev(ctypes.c_void_p(dev_a.data_ptr()), n, ctypes.byref(o32), ctypes.byref(r32)))
+            ks.append(r32.kernel_s)
+        t32 = statistics.median(ks)
+        f32 = {"ms_per_step": t32 * 1e3, "gray_steps_per_s": n * 2 ** (n - 1) / t32,
+               "rel_err_vs_exact": err_vs_exact(complex(r32.value, r32.imag)),
+               "timing": "walk kernel events, median of 5 (FP32 products, double-double unit bases and sum)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -406,6 +431,8 @@ def ours_arm(args, wl):
                     "d2h_bytes_per_step": 16 * comps + 4},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
             "gpu_launches": launches}
+    if f32 is not None:
+        line["fp32_products"] = f32
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -47,7 +47,12 @@ enum spb_status {
  * and SPB_PREC_DD to `calculation_precision=dd`. */
 enum spb_precision {
     SPB_PREC_FP64 = 0, /* FP64 row sums and products, double-double sum      */
-    SPB_PREC_DD = 1    /* + double-double re-evaluation of dominant units    */
+    SPB_PREC_DD = 1,   /* + double-double re-evaluation of dominant units    */
+    SPB_PREC_FP32 = 2  /* FP32 row sums and products (double-double unit
+                          bases and sum), n <= 40: about twice the FP64
+                          rate, relative error of order kappa * n * 2^-24;
+                          for inputs where that is within the caller's
+                          bound                                            */
 };
 
 /* Walk used by spb_perm_sparse_f64. */

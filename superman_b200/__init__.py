@@ -20,7 +20,7 @@ from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
 __all__ = ["Result", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "perm_approx",
            "approx_samples", "SupermanError", "SPB_PREC_FP64", "SPB_PREC_DD", "device_count"]
 
-_PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD}
+_PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD, "fp32": 2}
 _SPARSE_WALK = {"auto": 0, "never": 1, "always": 2}
 
 

@@ -29,6 +29,7 @@ SPB_ERR_NOT_SQUARE = 10
 # enum spb_precision
 SPB_PREC_FP64 = 0
 SPB_PREC_DD = 1
+SPB_PREC_FP32 = 2
 
 
 class SupermanError(RuntimeError):

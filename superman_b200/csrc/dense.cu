@@ -86,6 +86,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
         size_t pos = (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
         pb.de_hi[pos] = s.hi;
         pb.de_lo[pos] = s.lo;
+        if (pb.de32) pb.de32[pos] = __double2float_rn(s.hi);
     }
     // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
     //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|.
@@ -177,6 +178,8 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     size_t terms = (size_t)1 << pb->w;
     size_t o_deh = take(sizeof(double) * terms * n * c);
     size_t o_del = take(sizeof(double) * terms * n * c);
+    const bool f32 = pb->f32 != 0;
+    size_t o_d32 = f32 ? take(sizeof(float) * terms * n * c) : 0;
     size_t o_mt = take(sizeof(double) * (size_t)(n - 1 - pb->w > 0 ? n - 1 - pb->w : 1) * n * c);
     size_t o_part = take(sizeof(dd) * (size_t)pb->grid * c);
     size_t o_tick = take(sizeof(unsigned) * 4);
@@ -211,6 +214,7 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
         pb->x0_lo = reinterpret_cast<double*>(base + o_x0l);
         pb->de_hi = reinterpret_cast<double*>(base + o_deh);
         pb->de_lo = reinterpret_cast<double*>(base + o_del);
+        pb->de32 = f32 ? reinterpret_cast<float*>(base + o_d32) : nullptr;
         pb->mt = reinterpret_cast<double*>(base + o_mt);
         pb->partials = reinterpret_cast<dd*>(base + o_part);
         pb->ticket = reinterpret_cast<unsigned*>(base + o_tick);
@@ -288,6 +292,14 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     pb.na = n;
     pb.comps = comps;
     pb.w = choose_unit_bits(n, comps, &opt);
+    if (opt.precision == SPB_PREC_FP32) {
+        if (n > kMaxF32N || n < 3) {
+            spb_set_error("FP32 products are offered for 3 <= n <= %d (got n=%d)", kMaxF32N, n);
+            return out->status = SPB_ERR_INVALID;
+        }
+        pb.f32 = 1;
+        plan = nullptr;  // the FP32 variant is the dense walk
+    }
     if (plan && plan->na < n) {
         if (comps != 1 || plan->na < 1 || plan->na > kMaxActive || plan->w < 2 || plan->w > n - 2) {
             spb_set_error("row-compacted walk: bad plan (n=%d, active rows %d, w=%d)", n, plan->na, plan->w);
@@ -299,17 +311,18 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     pb.g = group_size(n, comps);
     pb.units = 1ull << (n - 1 - pb.w);
 
+    auto smem_for = [&](int th) { return pb.f32 ? walk_f32_smem_bytes(pb, th) : walk_smem_bytes(pb, th); };
     int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 0;
-    const int max_threads = pb.na < n ? 512 : walk_max_threads(n, comps);
+    const int max_threads = pb.f32 ? walk_f32_max_threads(n, comps) : (pb.na < n ? 512 : walk_max_threads(n, comps));
     if (threads == 0) {
         threads = max_threads;
         // fit the per-thread lo vectors next to the tables
-        while (threads > 64 && walk_smem_bytes(pb, threads) > ctx->smem_optin) threads -= 32;
+        while (threads > 64 && smem_for(threads) > ctx->smem_optin) threads -= 32;
     }
     if (threads > max_threads) threads = max_threads;
     threads = (threads / 32) * 32;
     if (threads < 32) threads = 32;
-    size_t smem = walk_smem_bytes(pb, threads);
+    size_t smem = smem_for(threads);
     if (smem > ctx->smem_optin) {
         spb_set_error("dense n=%d: %zu B shared memory exceeds the %zu B limit", n, smem, ctx->smem_optin);
         return out->status = SPB_ERR_INVALID;
@@ -358,7 +371,7 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     } else if (dd_mode) {  // 0x7f7f7f7f: above every bin
         SPB_CUDA_TRY(cudaMemsetAsync(pb.list_bin, 0x7f, sizeof(int), stream));
     }
-    st = launch_walk(pb, blocks, threads, smem, stream);
+    st = pb.f32 ? launch_walk_f32(pb, blocks, threads, smem, stream) : launch_walk(pb, blocks, threads, smem, stream);
     if (st != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
 

@@ -23,6 +23,8 @@ struct Problem {
     double* x0_lo;
     double* de_hi;             // [comps][2^w/G][n][G] low-column subset sums
     double* de_lo;             // rounding residues of de_hi
+    float* de32;               // SPB_PREC_FP32: de_hi rounded to float (else null)
+    int f32;                   // 1: the FP32-product walk runs (tables include de32)
     double* mt;                // [comps][n-1-w][n] high columns
     dd* partials;              // [comps][grid] per-CTA sums
     unsigned* ticket;          // last-CTA election counter (reset by the kernel)
@@ -580,6 +582,12 @@ int launch_collect(const Problem& pb, cudaStream_t s);
 // Lists the units whose bin >= pb.thr_bin from the walk's per-thread maxima
 // (pb.tmax), one warp per thread range, bases rebuilt from scratch.
 int launch_scan_parallel(const Problem& pb, cudaStream_t s);
+
+// FP32-product walks (f32_impl.cuh), n <= kMaxF32N.
+constexpr int kMaxF32N = 40;
+int launch_walk_f32(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+size_t walk_f32_smem_bytes(const Problem& pb, int threads);
+int walk_f32_max_threads(int n, int comps);
 
 // Per-n dispatch (defined in the instantiation units).
 int launch_walk_real(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
