@@ -86,8 +86,10 @@ typedef struct spb_result {
     double kernel_s;       /* device time of the Gray-walk kernels          */
     double device_s;       /* device time of the whole call on its stream:
                               input copy (if any), kernels, result copy     */
-    double err_est;        /* estimated relative error (statistical)        */
-    uint64_t gray_steps;   /* Gray steps walked: n*2^(n-1) (NW) or n*2^n    */
+    double err_est;        /* estimated relative error (statistical); for
+                              spb_perm_approx the relative standard error */
+    uint64_t gray_steps;   /* Gray steps walked, n*2^(n-1) (every walk is
+                              Nijenhuis-Wilf); spb_perm_approx: samples    */
     uint64_t refined_units;/* units re-evaluated in double-double           */
     int status;            /* enum spb_status                               */
     int launches;          /* kernels launched by the call                  */
