@@ -27,6 +27,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "context.h"
 #include "dense_host.h"
@@ -38,17 +39,22 @@ namespace spb {
 namespace dense {
 
 // ------------------------------------------------------------ setup kernel --
-// One CTA builds every table the walk kernels read.
+// One CTA builds every table the walk kernels read.  The matrix is staged in
+// shared memory (dynamic, n*n*comps doubles: setup_smem_bytes), so the table
+// builds below read it at shared-memory latency.
 __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
 {
     const int n = pb.n, c = pb.comps, w = pb.w, G = pb.g;
     const int tid = threadIdx.x, bd = blockDim.x;
     __shared__ int s_exp[kMaxN];
+    extern __shared__ double s_as[];  // [n][n][c], row-scaled after step 1
 
+    for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
+    __syncthreads();
     // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in [0.5, 1).
     for (int r = tid; r < n; r += bd) {
         double mx = 0.0;
-        for (int j = 0; j < n * c; ++j) mx = fmax(mx, fabs(a_in[(size_t)r * n * c + j]));
+        for (int j = 0; j < n * c; ++j) mx = fmax(mx, fabs(s_as[r * n * c + j]));
         int e = 0;
         if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
         s_exp[r] = e;
@@ -56,7 +62,9 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
     __syncthreads();
     for (int idx = tid; idx < n * n * c; idx += bd) {
         int r = idx / (n * c);
-        pb.as[idx] = ldexp(a_in[idx], -s_exp[r]);
+        const double v = ldexp(s_as[idx], -s_exp[r]);
+        s_as[idx] = v;
+        pb.as[idx] = v;
     }
     __syncthreads();
     if (tid == 0) {
@@ -68,25 +76,39 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
     for (int rr = tid; rr < n * c; rr += bd) {
         int r = rr / c, part = rr % c;
         dd s = {0.0, 0.0};
-        for (int j = 0; j < n; ++j) s = dd_add_d(s, pb.as[((size_t)r * n + j) * c + part]);
+        for (int j = 0; j < n; ++j) s = dd_add_d(s, s_as[(r * n + j) * c + part]);
         dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
-        dd x = dd_add_d(h, pb.as[((size_t)r * n + (n - 1)) * c + part]);
+        dd x = dd_add_d(h, s_as[(r * n + (n - 1)) * c + part]);
         pb.x0_hi[part * n + r] = x.hi;
         pb.x0_lo[part * n + r] = x.lo;
     }
-    // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per part.
+    // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per part:
+    //    the double-double sum of the selected columns added in ascending
+    //    order.  Built level by level: with k the highest bit of d,
+    //    DE[d] = DE[d - 2^k] + a_k, the same operations in the same order.
     const int terms = 1 << w;
-    for (int idx = tid; idx < terms * n * c; idx += bd) {
-        int part = idx / (terms * n);
-        int rem = idx % (terms * n);
-        int d = rem / n, r = rem % n;
-        dd s = {0.0, 0.0};
-        for (int j = 0; j < w; ++j)
-            if ((d >> j) & 1) s = dd_add_d(s, pb.as[((size_t)r * n + j) * c + part]);
-        size_t pos = (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
-        pb.de_hi[pos] = s.hi;
-        pb.de_lo[pos] = s.lo;
-        if (pb.de32) pb.de32[pos] = __double2float_rn(s.hi);
+    auto de_pos = [&](int part, int d, int r) {
+        return (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
+    };
+    for (int idx = tid; idx < n * c; idx += bd) {
+        const size_t pos = de_pos(idx / n, 0, idx % n);
+        pb.de_hi[pos] = 0.0;
+        pb.de_lo[pos] = 0.0;
+        if (pb.de32) pb.de32[pos] = 0.0f;
+    }
+    for (int k = 0; k < w; ++k) {
+        __syncthreads();  // level k reads the entries of levels < k
+        const int half = 1 << k;
+        for (int idx = tid; idx < half * n * c; idx += bd) {
+            const int part = idx / (half * n), rem = idx % (half * n);
+            const int d = half + rem / n, r = rem % n;
+            const size_t from = de_pos(part, d - half, r);
+            const dd s = dd_add_d(dd{pb.de_hi[from], pb.de_lo[from]}, s_as[(r * n + k) * c + part]);
+            const size_t pos = de_pos(part, d, r);
+            pb.de_hi[pos] = s.hi;
+            pb.de_lo[pos] = s.lo;
+            if (pb.de32) pb.de32[pos] = __double2float_rn(s.hi);
+        }
     }
     // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
     //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|.
@@ -99,7 +121,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
         for (int r = tid; r < n; r += bd) {
             double lo = 0.0, hi = 0.0;
             for (int j = 0; j < w; ++j) {
-                double v = pb.as[(size_t)r * n + j];
+                double v = s_as[r * n + j];
                 if (v < 0.0) lo += v; else hi += v;
             }
             pb.bnd[r] = lo;
@@ -121,7 +143,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
         int part = idx / (ntop * n);
         int rem = idx % (ntop * n);
         int j = rem / n, r = rem % n;
-        pb.mt[idx] = pb.as[((size_t)r * n + (w + j)) * c + part];
+        pb.mt[idx] = s_as[(r * n + (w + j)) * c + part];
         (void)part;
     }
 }
@@ -134,6 +156,28 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
 // ======================================================================
 namespace spb {
 namespace dense {
+
+size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
+
+int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s)
+{
+    // up to 63*63*2 doubles (63.5 KB) of staged matrix: raise the dynamic limit once per device
+    static std::mutex mu;
+    static bool done[64] = {false};
+    int dev = 0;
+    SPB_CUDA_TRY(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!done[dev & 63]) {
+            SPB_CUDA_TRY(cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)setup_smem_bytes(kMaxN, 2)));
+            done[dev & 63] = true;
+        }
+    }
+    setup_kernel<<<1, 512, setup_smem_bytes(pb.n, pb.comps), s>>>(pb, d_a);
+    SPB_CUDA_TRY(cudaGetLastError());
+    return SPB_OK;
+}
 
 // Terms per group in the walk kernels; must equal RealCfg<N>::G /
 // ComplexCfg<N>::G, and the unit (2^w terms) must hold at least one group.
@@ -357,11 +401,14 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         SPB_CUDA_TRY(cudaMemsetAsync(pb.pre_cnt, 0, sizeof(unsigned) * kHistBins, stream));
         SPB_CUDA_TRY(cudaMemsetAsync(pb.raw_n, 0, sizeof(unsigned long long), stream));
     }
-    setup_kernel<<<1, 512, 0, stream>>>(pb, d_a);
+    if ((st = launch_setup(pb, d_a, stream)) != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaGetLastError());
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
     int launches = 2;
-    if (dd_mode && pb.na == n) {
+    if (dd_mode && pb.na == n && pb.units <= pb.raw_cap / 2) {
+        // every unit fits the list: list them all (bin 0 and up), no bound pass
+        SPB_CUDA_TRY(cudaMemsetAsync(pb.list_bin, 0, sizeof(int), stream));
+    } else if (dd_mode && pb.na == n) {
         // Size the first pass's unit list from a bound-only pass (about 1.5 %
         // of a dense walk).  The row-compacted walk has few terms per unit, so
         // there the pass would cost a large share; it lists nothing and a

@@ -38,6 +38,7 @@ namespace spb {
 namespace dense {
 // Defined in dense.cu.
 __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in);
+int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s);
 int group_size(int n, int comps);
 int choose_unit_bits(int n, int comps, const spb_options* opt);
 size_t plan_layout(Problem* pb, char* base, size_t* in_offset);
@@ -138,8 +139,8 @@ extern "C" int spb_perm_dense_f64_noalloc(const double* d_a, int n, double* d_ou
 
     // The ticket must start at zero; everything else is overwritten.
     SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, s));
-    setup_kernel<<<1, 512, 0, s>>>(pb, d_a);
-    SPB_CUDA_TRY(cudaGetLastError());
+    int st0 = launch_setup(pb, d_a, s);
+    if (st0 != SPB_OK) return st0;
     int st = launch_walk(pb, blocks, threads, smem, s);
     if (st != SPB_OK) return st;
     noalloc_finalize<<<1, 32, 0, s>>>(pb, d_out);
