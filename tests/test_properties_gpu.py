@@ -118,3 +118,24 @@ def test_injected_failure_in_server_create(spb):
         a = W.dense_uniform(10, 1)
         got = srv.wait(srv.submit(a))["permanent"]
         assert abs(got - spb.perm_dense(a).permanent) <= 1e-13 * abs(got)
+
+
+def test_edge_values(spb):
+    """Zeros give exactly 0; a permanent beyond the double range comes back
+    infinite and a NaN entry gives NaN (the reference prints such results as
+    'overflowed', main.cpp:122-125); rows are scaled by powers of two, so
+    entries near the range limits alone do not overflow the walk."""
+    assert spb.perm_dense(np.zeros((12, 12))).permanent == 0.0
+    z = W.dense_uniform(22, 5)
+    z[7] = 0.0
+    assert spb.perm_dense(z).permanent == 0.0
+    big = np.full((20, 20), 1e300)
+    assert np.isinf(spb.perm_dense(big).permanent)
+    tiny = np.full((12, 12), 1e-300)  # 12! * 1e-3600 underflows to 0
+    assert spb.perm_dense(tiny).permanent == 0.0
+    scaled = np.full((12, 12), 2.0 ** 900)  # rows far from 1, result in range
+    r = spb.perm_dense(scaled / 2.0 ** 900 * 0.75)
+    assert abs(r.permanent - math.factorial(12) * 0.75 ** 12) <= 1e-13 * r.permanent
+    nan = W.dense_uniform(10, 6)
+    nan[3, 4] = np.nan
+    assert np.isnan(spb.perm_dense(nan).permanent)
