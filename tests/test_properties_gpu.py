@@ -133,8 +133,11 @@ def test_edge_values(spb):
     assert np.isinf(spb.perm_dense(big).permanent)
     tiny = np.full((12, 12), 1e-300)  # 12! * 1e-3600 underflows to 0
     assert spb.perm_dense(tiny).permanent == 0.0
-    scaled = np.full((12, 12), 2.0 ** 900)  # rows far from 1, result in range
-    r = spb.perm_dense(scaled / 2.0 ** 900 * 0.75)
+    # rows at 2^900 and 2^-900 whose scales cancel: the result is in range
+    scaled = np.full((12, 12), 0.75)
+    scaled[:6] *= 2.0 ** 900
+    scaled[6:] *= 2.0 ** -900
+    r = spb.perm_dense(scaled)
     assert abs(r.permanent - math.factorial(12) * 0.75 ** 12) <= 1e-13 * r.permanent
     nan = W.dense_uniform(10, 6)
     nan[3, 4] = np.nan
