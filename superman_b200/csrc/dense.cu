@@ -25,6 +25,7 @@
 // exponent sum is applied to the final result.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -227,12 +228,10 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     size_t o_mt = take(sizeof(double) * (size_t)(n - 1 - pb->w > 0 ? n - 1 - pb->w : 1) * n * c);
     size_t o_part = take(sizeof(dd) * (size_t)pb->grid * c);
     size_t o_tick = take(sizeof(unsigned) * 4);
-    size_t o_res = take(sizeof(dd) * 2);
-    size_t o_exp = take(sizeof(int) * 4);
+    size_t o_rbk = take(sizeof(Readback));
     size_t o_bnd = take(sizeof(double) * 2 * n);
     size_t o_hs = take(sizeof(double) * kHistBins);
     size_t o_hc = take(sizeof(unsigned long long) * kHistBins);
-    size_t o_ln = take(sizeof(unsigned long long) * 2);
     const size_t T = (size_t)pb->grid * pb->threads;
     const bool refine = pb->mode != 0;
     size_t o_tm = refine ? take(sizeof(unsigned short) * T) : 0;
@@ -252,7 +251,6 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
         pb->bnd = reinterpret_cast<double*>(base + o_bnd);
         pb->hist_s2 = reinterpret_cast<double*>(base + o_hs);
         pb->hist_cnt = reinterpret_cast<unsigned long long*>(base + o_hc);
-        pb->list_n = reinterpret_cast<unsigned long long*>(base + o_ln);
         pb->as = reinterpret_cast<double*>(base + o_as);
         pb->x0_hi = reinterpret_cast<double*>(base + o_x0h);
         pb->x0_lo = reinterpret_cast<double*>(base + o_x0l);
@@ -262,8 +260,10 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
         pb->mt = reinterpret_cast<double*>(base + o_mt);
         pb->partials = reinterpret_cast<dd*>(base + o_part);
         pb->ticket = reinterpret_cast<unsigned*>(base + o_tick);
-        pb->result = reinterpret_cast<dd*>(base + o_res);
-        pb->exp_sum = reinterpret_cast<int*>(base + o_exp);
+        pb->rb = reinterpret_cast<Readback*>(base + o_rbk);
+        pb->result = pb->rb->res;
+        pb->exp_sum = &pb->rb->exp_sum;
+        pb->list_n = &pb->rb->list_n;
     }
     if (in_offset) *in_offset = o_in;
     return off;
@@ -278,35 +278,6 @@ size_t walk_smem_bytes(const Problem& pb, int threads)
     return sizeof(double) * (terms * n * c + (size_t)(ntop > 0 ? ntop : 0) * n * c +
                              (size_t)n * c * threads) +
            kHistSmemBytes + bound_smem_bytes(n);
-}
-
-// Picks the histogram bin (bins are keyed by each unit's bound U and hold the
-// units' actual sums of squared terms) from which units are re-evaluated in
-// double-double: the unrefined units' expected FP64 rounding error,
-// sqrt(sum t^2 * k/12) * 2^-52 with k rounded operations per term, must stay
-// below half the tolerance relative to the first-pass magnitude.  At most 1/8
-// of the units are refined; past that the estimate is reported instead.
-// Returns the bin; sets *count (units to refine) and *err_est.
-static int pick_threshold(const double* s2, const unsigned long long* cnt, int n, int comps,
-                          double mag, double tol, unsigned long long units,
-                          unsigned long long* count, double* err_est)
-{
-    const double k = comps == 1 ? 2.0 * n : 6.0 * n;
-    const double var_per_s2 = k / 12.0 * std::ldexp(1.0, -104);
-    const double budget = mag > 0.0 ? (0.5 * tol * mag) * (0.5 * tol * mag) : 0.0;
-    double cum = 0.0;
-    int b = 0;
-    while (b < kHistBins && cum + s2[b] * var_per_s2 <= budget) cum += s2[b++] * var_per_s2;
-    unsigned long long c = 0;
-    for (int i = b; i < kHistBins; ++i) c += cnt[i];
-    while (c > units / 8 && b < kHistBins) {
-        cum += s2[b] * var_per_s2;
-        c -= cnt[b];
-        ++b;
-    }
-    *count = c;
-    *err_est = mag > 0.0 ? std::sqrt(cum) / mag : INFINITY;
-    return b;
 }
 
 int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in, spb_result* out,
@@ -386,6 +357,20 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     if ((st = ensure_scratch(ctx, need)) != SPB_OK) return out->status = st;
     char* base = static_cast<char*>(ctx->scratch);
     plan_layout(&pb, base, &in_off);
+    if ((st = ensure_pinned(ctx, sizeof(Readback))) != SPB_OK) return out->status = st;
+    Readback* hrb = static_cast<Readback*>(ctx->pinned);
+    // The refinement list is sized before the walk for the threshold's cap
+    // (1/8 of the units), up to 2^21 units; a larger count is met after the
+    // readback with a larger list.
+    const size_t entry = sizeof(double) * 2 * n * comps;
+    if (dd_mode) {
+        const unsigned long long cap = std::min<unsigned long long>(pb.units / 8 + 1, 1ull << 21);
+        if ((st = ensure_list(ctx, cap * sizeof(unsigned long long) + 256)) != SPB_OK) return out->status = st;
+        pb.list_u = static_cast<unsigned long long*>(ctx->list);
+        pb.list_cap = cap;
+        pb.list_x = nullptr;
+        pb.tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
+    }
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
     const double* d_a = a;
     if (!a_on_device) {
@@ -422,99 +407,96 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     if (st != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
 
-    struct {
-        dd res[2];
-        int e;
-    } h;
-    SPB_CUDA_TRY(cudaMemcpyAsync(h.res, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
-    SPB_CUDA_TRY(cudaMemcpyAsync(&h.e, pb.exp_sum, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    double ms_refine = 0.0;
-    if (dd_mode) {
-        // First pass done: read its total and the unit histogram.
-        static thread_local double hs2[kHistBins];
-        static thread_local unsigned long long hcnt[kHistBins];
-        int list_bin = kHistBins;
-        unsigned long long raw_n = 0;
-        SPB_CUDA_TRY(cudaMemcpyAsync(hs2, pb.hist_s2, sizeof(hs2), cudaMemcpyDeviceToHost, stream));
-        SPB_CUDA_TRY(cudaMemcpyAsync(hcnt, pb.hist_cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, stream));
-        SPB_CUDA_TRY(cudaMemcpyAsync(&list_bin, pb.list_bin, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        SPB_CUDA_TRY(cudaMemcpyAsync(&raw_n, pb.raw_n, sizeof(raw_n), cudaMemcpyDeviceToHost, stream));
+    // Double-double: threshold, listing and refinement follow the walk on the
+    // stream; the host reads everything back once.
+    auto enqueue_refinement = [&]() -> int {
+        int r;
+        if ((r = launch_listing(pb, stream)) != SPB_OK) return r;
+        if ((r = launch_refine(pb, blocks, stream)) != SPB_OK) return r;
+        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref1, stream));
+        launches += 2;
+        return SPB_OK;
+    };
+    auto read_back = [&]() -> int {
+        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
+        SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
         SPB_CUDA_TRY(cudaStreamSynchronize(stream));
-        const double tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
-        const double mag = comps == 1 ? std::fabs(h.res[0].hi) : std::hypot(h.res[0].hi, h.res[1].hi);
-        unsigned long long count = 0;
-        double err = 0.0;
-        const int thr = pick_threshold(hs2, hcnt, n, comps, mag, tol, pb.units, &count, &err);
-        out->err_est = err;
-        if (count > 0) {
-            const size_t entry = sizeof(double) * 2 * n * comps;
-            if ((st = ensure_list(ctx, count * (entry + sizeof(unsigned long long)) + 256)) != SPB_OK)
-                return out->status = st;
-            pb.thr_bin = thr;
-            pb.list_cap = count;
-            pb.list_u = static_cast<unsigned long long*>(ctx->list);
-            unsigned long long listed = 0;
-            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
-            // Fast path: the first pass listed every unit at or above list_bin;
-            // when the threshold is not below it and the list did not
-            // overflow, the units to refine are all in that list.
-            // Otherwise a parallel scan lists them (bases rebuilt from scratch).
-            // Both are checked against the histogram's count; the replay scan
-            // below, whose bases are the walk's own, is the last resort.
-            const bool from_list = thr >= list_bin && raw_n <= pb.raw_cap;
-            bool fast = false;
-            if (!opt.replay_listing) {
-                pb.list_x = nullptr;
-                SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
-                st = from_list ? launch_collect(pb, stream) : launch_scan_parallel(pb, stream);
-                if (st != SPB_OK) return out->status = st;
-                SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
-                SPB_CUDA_TRY(cudaStreamSynchronize(stream));
-                fast = listed == count;
-                launches += 1;
-            }
-            if (!fast) {  // replay the walk and list the units with their bases
-                pb.mode = 2;
-                pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
-                                                      align_up(count * sizeof(unsigned long long), 256));
-                SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
-                if ((st = launch_walk(pb, blocks, threads, smem, stream)) != SPB_OK) return out->status = st;
-                launches += 1;
-            }
-            if ((st = launch_refine(pb, count, blocks, stream)) != SPB_OK) return out->status = st;
-            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref1, stream));
-            launches += 1;
-            dd corr[2];
-            SPB_CUDA_TRY(cudaMemcpyAsync(corr, pb.result, sizeof(dd) * comps, cudaMemcpyDeviceToHost, stream));
-            SPB_CUDA_TRY(cudaMemcpyAsync(&listed, pb.list_n, sizeof(listed), cudaMemcpyDeviceToHost, stream));
-            SPB_CUDA_TRY(cudaStreamSynchronize(stream));
-            if (listed != count) {
-                spb_set_error("refinement listed %llu units, histogram counted %llu",
-                              (unsigned long long)listed, (unsigned long long)count);
-                return out->status = SPB_ERR_CUDA;
-            }
-            out->refined_units = count;
-            for (int cc = 0; cc < comps; ++cc) h.res[cc] = dd_add(h.res[cc], corr[cc]);
-            float mr = 0.f;
-            SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
-            ms_refine = mr;
-            out->refined_units = count;
+        return SPB_OK;
+    };
+    bool refined = false;
+    if (dd_mode) {
+        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
+        if ((st = launch_threshold(pb, stream)) != SPB_OK) return out->status = st;
+        launches += 1;
+        if (!opt.replay_listing) {
+            if ((st = enqueue_refinement()) != SPB_OK) return out->status = st;
+            refined = true;
         }
     }
-    SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
-    SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+    if ((st = read_back()) != SPB_OK) return out->status = st;
+    const dd res0[2] = {hrb->res[0], hrb->res[1]};
+    dd res[2] = {res0[0], res0[1]};
+    const int exp_sum = hrb->exp_sum;
+    double ms_refine = 0.0;
+    if (dd_mode) {
+        const unsigned long long count = hrb->count;
+        out->err_est = hrb->err;
+        bool ok = refined && hrb->list_n == count && count <= pb.list_cap;
+        if (!ok && refined && count > pb.list_cap) {
+            // more units than the list was sized for: the same listing, larger list
+            if ((st = ensure_list(ctx, count * sizeof(unsigned long long) + 256)) != SPB_OK)
+                return out->status = st;
+            pb.list_u = static_cast<unsigned long long*>(ctx->list);
+            pb.list_cap = count;
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
+            SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+            if ((st = enqueue_refinement()) != SPB_OK) return out->status = st;
+            if ((st = read_back()) != SPB_OK) return out->status = st;
+            ok = hrb->list_n == count;
+        }
+        if (!ok) {
+            // Replay the walk (mode 2, same launch shape, so the unit bases
+            // are the walk's own) and list the units with their bases.
+            if ((st = ensure_list(ctx, count * (entry + sizeof(unsigned long long)) + 256)) != SPB_OK)
+                return out->status = st;
+            pb.mode = 2;
+            pb.thr_bin = hrb->thr;
+            pb.list_cap = count;
+            pb.list_u = static_cast<unsigned long long*>(ctx->list);
+            pb.list_x = reinterpret_cast<double*>(static_cast<char*>(ctx->list) +
+                                                  align_up(count * sizeof(unsigned long long), 256));
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref0, stream));
+            SPB_CUDA_TRY(cudaMemsetAsync(pb.list_n, 0, sizeof(unsigned long long), stream));
+            if (count > 0 && (st = launch_walk(pb, blocks, threads, smem, stream)) != SPB_OK)
+                return out->status = st;
+            if ((st = launch_refine(pb, blocks, stream)) != SPB_OK) return out->status = st;
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_ref1, stream));
+            launches += count > 0 ? 2 : 1;
+            if ((st = read_back()) != SPB_OK) return out->status = st;
+            if (hrb->list_n != count) {
+                spb_set_error("refinement listed %llu units, histogram counted %llu",
+                              (unsigned long long)hrb->list_n, (unsigned long long)count);
+                return out->status = SPB_ERR_CUDA;
+            }
+        }
+        for (int cc = 0; cc < comps; ++cc) res[cc] = dd_add(res0[cc], hrb->corr[cc]);
+        out->refined_units = count;
+        float mr = 0.f;
+        SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
+        ms_refine = mr;
+    }
     float ms = 0.f, ms_call = 0.f;
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));
 
     // perm = (4(n%2)-2) * total * 2^E ; the factor is +-2, an exact power of two.
-    const int e = h.e + 1;
+    const int e = exp_sum + 1;
     const double sgn = (n % 2) ? 1.0 : -1.0;
-    out->value = sgn * std::ldexp(h.res[0].hi, e);
-    out->value_lo = sgn * std::ldexp(h.res[0].lo, e);
+    out->value = sgn * std::ldexp(res[0].hi, e);
+    out->value_lo = sgn * std::ldexp(res[0].lo, e);
     if (comps == 2) {
-        out->imag = sgn * std::ldexp(h.res[1].hi, e);
-        out->imag_lo = sgn * std::ldexp(h.res[1].lo, e);
+        out->imag = sgn * std::ldexp(res[1].hi, e);
+        out->imag_lo = sgn * std::ldexp(res[1].lo, e);
     }
     out->kernel_s = (ms + ms_refine) * 1e-3;
     out->device_s = ms_call * 1e-3;

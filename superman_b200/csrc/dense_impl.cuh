@@ -11,6 +11,21 @@ namespace dense {
 
 constexpr int kMaxN = 63;
 
+// Everything the host reads back after a call, contiguous so that one copy
+// brings it over: a call costs one host round trip, the double-double
+// refinement included (its threshold is picked on the device).
+struct Readback {
+    dd res[2];                  // [comps] the walk's total
+    dd corr[2];                 // [comps] the refinement's correction
+    unsigned long long list_n;  // units listed for the refinement
+    unsigned long long count;   // units the histogram puts at or above thr
+    double err;                 // expected relative error of the unrefined units
+    int thr;                    // refinement bin
+    int from_list;              // 1: the walk's own list holds every unit at or above thr
+    int exp_sum;                // sum of the row scaling exponents
+    int pad;
+};
+
 // Device-side description of one permanent: sizes plus pointers into the
 // scratch arena written by setup_kernel.
 struct Problem {
@@ -28,15 +43,17 @@ struct Problem {
     double* mt;                // [comps][n-1-w][n] high columns
     dd* partials;              // [comps][grid] per-CTA sums
     unsigned* ticket;          // last-CTA election counter (reset by the kernel)
-    dd* result;                // [comps] grid total
-    int* exp_sum;              // sum of the row scaling exponents
+    dd* result;                // [comps] grid total (rb->res; rb->corr for the refinement)
+    int* exp_sum;              // sum of the row scaling exponents (&rb->exp_sum)
+    Readback* rb;
+    double tol;                // SPB_PREC_DD: relative tolerance of the threshold
     // Double-double refinement (SPB_PREC_DD); unused when mode == 0.
     int mode;                  // 0 walk, 1 walk + unit-bound histogram, 2 scan only
     int thr_bin;               // mode 2: list the units whose bound bin >= thr_bin
     double* bnd;               // real [2][n] min/max of DE over d; complex [n] max |DE|
     double* hist_s2;           // [kHistBins] sum of squared terms of the units per bin
     unsigned long long* hist_cnt;  // [kHistBins] units per bin
-    unsigned long long* list_n;    // mode 2: number of listed units
+    unsigned long long* list_n;    // number of listed units (&rb->list_n)
     unsigned long long list_cap;
     unsigned long long* list_u;    // [list_cap] unit index
     double* list_x;                // [list_cap][comps][2][n] unit base, hi then lo
@@ -568,20 +585,26 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     if (mode != 2) grid_reduce<2>(tot, pb);
 }
 
-// Re-evaluates the units listed by a mode-2 scan in double-double and
-// accumulates (double-double unit sum - the walk's FP64 unit sum) into
-// pb.result, one warp per unit.  Defined in dense_refine.cu.
-int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s);
-
-// Mode-1 listing support (dense_refine.cu): bound_walk + pick_list_bin run
-// before the walk; collect then keeps the listed units whose bin >=
-// pb.thr_bin (pb.list_u, count in *pb.list_n), and the refine kernel
-// rebuilds each unit base from scratch (pb.list_x == nullptr).
+// Double-double refinement (dense_refine.cu), all stream-ordered after the
+// mode-1 walk with no host round trip in between:
+//   launch_threshold   picks rb->thr / rb->count / rb->err from the
+//                      histogram and decides the listing path (rb->from_list);
+//   launch_listing     lists the units whose bin >= rb->thr: from the walk's
+//                      own list when rb->from_list, else from the walk's
+//                      per-thread maxima (pb.tmax), one warp per thread
+//                      range, bases rebuilt from scratch;
+//   launch_refine      re-evaluates the listed units in double-double and
+//                      writes sum(double-double unit sum - the walk's FP64
+//                      unit sum) to rb->corr, one warp per unit; it refines
+//                      nothing unless rb->list_n == rb->count <= pb.list_cap.
+// bound_walk + pick_list_bin run before the walk and set the bin from which
+// the walk lists its units.  A mode-2 walk (same launch shape as mode 1)
+// replays the listing with the walk's own bases (pb.list_x) when the host
+// finds the count check failed.
+int launch_threshold(const Problem& pb, cudaStream_t s);
+int launch_refine(const Problem& pb, int blocks, cudaStream_t s);
 int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s);
-int launch_collect(const Problem& pb, cudaStream_t s);
-// Lists the units whose bin >= pb.thr_bin from the walk's per-thread maxima
-// (pb.tmax), one warp per thread range, bases rebuilt from scratch.
-int launch_scan_parallel(const Problem& pb, cudaStream_t s);
+int launch_listing(const Problem& pb, cudaStream_t s);
 
 // FP32-product walks (f32_impl.cuh), n <= kMaxF32N.
 constexpr int kMaxF32N = 40;

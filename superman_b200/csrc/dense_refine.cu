@@ -5,11 +5,11 @@
 // full set).  Their FP64 rounding errors, not the many small terms, set the
 // final error.  The walk (mode 1) bins every unit by an upper bound U_u of its
 // terms and accumulates the unit's actual sum of squared terms in that bin;
-// the host picks the bin from which the remaining units' rounding error fits
-// the tolerance.  The units at or above it come from the walk's own list
+// dd_threshold picks the bin from which the remaining units' rounding error
+// fits the tolerance.  The units at or above it come from the walk's own list
 // (every unit at or above a bin chosen beforehand by bound_walk, when that
-// bin is low enough), else from a parallel scan (scan_parallel), and only if
-// either count disagrees with the histogram from a replay scan (walk mode 2,
+// bin is low enough), else from a parallel scan (list_units does either), and
+// only if either count disagrees with the histogram from a replay scan (walk mode 2,
 // same launch shape, so the unit bases are bit-identical) that lists them
 // with their double-double base vectors.  This kernel then re-evaluates each
 // listed unit, one warp per unit:
@@ -20,6 +20,8 @@
 // and accumulates sign_u * (dd_sum - fp64_sum) into pb.result.  Adding that
 // correction to the walk's total replaces the dominant units' FP64 values by
 // their double-double values.
+#include <mutex>
+
 #include "bound_impl.cuh"
 #include "dense_impl.cuh"
 
@@ -97,14 +99,14 @@ __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const dou
 
 // Unit base of unit u (component `part`) rebuilt from scratch in
 // double-double the way the walk builds a thread's first unit (x0 plus the
-// selected high columns in index order); lanes take rows.
-__device__ __forceinline__ void unit_base(const Problem& pb, unsigned long long u, int part, int lane, double* hi,
-                                          double* lo)
+// selected high columns in index order); the worker's threads take rows.
+__device__ __forceinline__ void unit_base(const Problem& pb, const double* mt_all, unsigned long long u, int part,
+                                          int lane, double* hi, double* lo, int stride = 32)
 {
     const int n = pb.n, ntop = n - 1 - pb.w;
     const unsigned long long g = gray_of(u);
-    const double* mt = pb.mt + (size_t)part * (ntop > 0 ? ntop : 0) * n;
-    for (int r = lane; r < n; r += 32) {
+    const double* mt = mt_all + (size_t)part * (ntop > 0 ? ntop : 0) * n;
+    for (int r = lane; r < n; r += stride) {
         dd x = {pb.x0_hi[part * n + r], pb.x0_lo[part * n + r]};
         for (int j = 0; j < ntop; ++j)
             if ((g >> j) & 1ull) x = dd_add_d(x, mt[j * n + r]);
@@ -137,18 +139,32 @@ __device__ double unit_bound_rt(const Problem& pb, const double* xh)
     return ub;
 }
 
-// Parallel listing of the units whose bin >= thr_bin.  The walk's threads
-// whose highest bin reaches it (tmax) are visited one per warp; each lane
+// Lists the units whose bin >= rb->thr, unit indices only (the refine kernel
+// rebuilds the bases).  When the walk's own list holds all of them
+// (rb->from_list), every thread keeps the listed units at or above rb->thr.
+// Otherwise the walk's threads whose highest bin reaches it (tmax) are
+// visited one per warp; each lane
 // takes a contiguous part of that thread's units, builds the first unit base
 // from scratch in double-double and steps through the Gray order with the
-// walk's own base update, evaluating the walk's bound per unit.  Lists unit
-// indices only (the refine kernel rebuilds the bases).  A lane's bases start
+// walk's own base update, evaluating the walk's bound per unit.  A lane's bases start
 // from a rebuild rather than from the walk's thread start, so a hi word could
 // in principle differ from the walk's (a row value within ~2^-100 of a
 // rounding midpoint); if that ever moved a unit across the threshold the
 // count check fails and the caller falls back to the replay scan.
-__global__ void __launch_bounds__(128) scan_parallel(Problem pb)
+__global__ void __launch_bounds__(128) list_units(Problem pb)
 {
+    if (pb.rb->count == 0) return;
+    const int thr = pb.rb->thr;
+    if (pb.rb->from_list) {
+        const unsigned long long m = *pb.raw_n < pb.raw_cap ? *pb.raw_n : pb.raw_cap;
+        for (unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; e < m;
+             e += (unsigned long long)gridDim.x * blockDim.x)
+            if ((int)pb.raw_b[e] >= thr) {
+                const unsigned long long i = atomicAdd(pb.list_n, 1ull);
+                if (i < pb.list_cap) pb.list_u[i] = pb.raw_u[e];
+            }
+        return;
+    }
     const unsigned long long T = (unsigned long long)pb.grid * pb.threads;
     const int lane = threadIdx.x & 31, n = pb.n, c = pb.comps;
     const int ntop = n - 1 - pb.w, ntp = ntop > 0 ? ntop : 0;
@@ -156,7 +172,7 @@ __global__ void __launch_bounds__(128) scan_parallel(Problem pb)
     const unsigned long long nwarps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
     double xh[2 * kMaxN], xl[2 * kMaxN];  // [comps][kMaxN], per lane
     for (unsigned long long t = warp; t < T; t += nwarps) {
-        if ((int)pb.tmax[t] < pb.thr_bin) continue;  // warp-uniform
+        if ((int)pb.tmax[t] < thr) continue;  // warp-uniform
         unsigned long long u0, u1;
         balanced_range(pb.units, T, t, &u0, &u1);
         unsigned long long a, b;
@@ -176,7 +192,7 @@ __global__ void __launch_bounds__(128) scan_parallel(Problem pb)
             }
         }
         for (unsigned long long u = a;;) {
-            if (hist_bin(unit_bound_rt(pb, xh)) >= pb.thr_bin) {
+            if (hist_bin(unit_bound_rt(pb, xh)) >= thr) {
                 const unsigned long long i = atomicAdd(pb.list_n, 1ull);
                 if (i < pb.list_cap) pb.list_u[i] = u;
             }
@@ -212,83 +228,251 @@ __global__ void pick_list_bin(Problem pb)
     }
 }
 
-// Keeps the mode-1 listed units whose bin >= thr_bin.
-__global__ void collect_listed(Problem pb)
+// Picks the refinement bin: the lowest bin b such that the units below it,
+// left in FP64, have an expected rounding error sqrt(sum t^2 * k/12) * 2^-52
+// (k rounded operations per term) within half the tolerance of the walk's
+// magnitude.  At most 1/8 of the units are refined; past that b moves up and
+// the estimate is reported instead.  Also decides whether the walk's own list
+// holds every unit at or above b (no overflow, b >= its list bin) and resets
+// the list counter.  One warp; lane l owns bins [16l, 16l + 16), and the
+// cumulative sums over bins are lane-local sums joined by warp scans (a fixed
+// order, so the result is deterministic).
+__global__ void __launch_bounds__(32) dd_threshold(Problem pb)
 {
-    const unsigned long long m = *pb.raw_n < pb.raw_cap ? *pb.raw_n : pb.raw_cap;
-    for (unsigned long long e = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; e < m;
-         e += (unsigned long long)gridDim.x * blockDim.x)
-        if ((int)pb.raw_b[e] >= pb.thr_bin) {
-            const unsigned long long i = atomicAdd(pb.list_n, 1ull);
-            if (i < pb.list_cap) pb.list_u[i] = pb.raw_u[e];
+    constexpr int kPer = kHistBins / 32;
+    const int lane = threadIdx.x;
+    const unsigned full = 0xffffffffu;
+    Readback* rb = pb.rb;
+    const double k = pb.comps == 1 ? 2.0 * pb.n : 6.0 * pb.n;
+    const double var_per_s2 = mul_rn(k / 12.0, 0x1p-104);
+    const double mag = pb.comps == 1 ? fabs(rb->res[0].hi) : hypot(rb->res[0].hi, rb->res[1].hi);
+    const double half = mul_rn(0.5 * pb.tol, mag);
+    const double budget = mag > 0.0 ? mul_rn(half, half) : 0.0;
+    double v[kPer];
+    unsigned long long cn[kPer];
+    double loc = 0.0;
+    unsigned long long cl = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        v[i] = mul_rn(pb.hist_s2[lane * kPer + i], var_per_s2);
+        cn[i] = pb.hist_cnt[lane * kPer + i];
+        loc = add_rn(loc, v[i]);
+        cl += cn[i];
+    }
+    // Inclusive prefix of the lanes' sums of v, inclusive suffix of their counts.
+    double incl = loc;
+    unsigned long long sfx = cl;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(full, incl, d);
+        const unsigned long long p = __shfl_down_sync(full, sfx, d);
+        if (lane >= d) incl = add_rn(incl, o);
+        if (lane + d < 32) sfx += p;
+    }
+    double excl = __shfl_up_sync(full, incl, 1);
+    if (lane == 0) excl = 0.0;
+    unsigned long long after = __shfl_down_sync(full, sfx, 1);  // units in the lanes above
+    if (lane == 31) after = 0;
+    // b0: the first bin whose cumulative sum would exceed the budget.
+    int first = kHistBins;
+    double cum = excl;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i)
+        if (first == kHistBins) {
+            const double next = add_rn(cum, v[i]);
+            if (!(next <= budget)) first = lane * kPer + i;
+            else cum = next;
         }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(full, first, d));
+    // b: the first bin >= b0 whose tail holds at most units/8 units.
+    const unsigned long long cap = pb.units / 8;
+    int bsel = kHistBins;
+    unsigned long long tail = after;  // units in bins >= the current one, walking down
+#pragma unroll
+    for (int i = kPer - 1; i >= 0; --i) {
+        tail += cn[i];
+        const int bin = lane * kPer + i;
+        if (bin >= first && tail <= cap) bsel = bin;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) bsel = min(bsel, __shfl_xor_sync(full, bsel, d));
+    // The owner of bin bsel (lane 31 for bsel == kHistBins) has the sums below it.
+    const int owner = bsel < kHistBins ? bsel / kPer : 31;
+    double below = excl;
+    unsigned long long from = after;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int bin = lane * kPer + i;
+        if (bin < bsel) below = add_rn(below, v[i]);
+        else from += cn[i];
+    }
+    below = __shfl_sync(full, below, owner);
+    from = __shfl_sync(full, from, owner);
+    if (lane == 0) {
+        rb->thr = bsel;
+        rb->count = bsel < kHistBins ? from : 0ull;
+        rb->err = mag > 0.0 ? sqrt(below) / mag : INFINITY;
+        rb->from_list = (bsel >= *pb.list_bin && *pb.raw_n <= pb.raw_cap) ? 1 : 0;
+        rb->list_n = 0;
+    }
 }
 
-__global__ void __launch_bounds__(256) refine_real(Problem pb, unsigned long long count)
+// Units to refine: the histogram's count when the listing found exactly
+// that many and the list held them all, else none (the host then lists
+// again and reruns the refinement).
+__device__ __forceinline__ unsigned long long refine_count(const Problem& pb)
 {
+    const unsigned long long want = pb.rb->count;
+    return (pb.rb->list_n == want && want <= pb.list_cap) ? want : 0ull;
+}
+
+// Copies m doubles from global to shared memory, eight loads in flight per
+// thread (a plain loop waits out one global-memory latency per element).
+__device__ __forceinline__ void stage(double* dst, const double* __restrict__ src, int m)
+{
+    const int bd = blockDim.x;
+    for (int i0 = threadIdx.x; i0 < m; i0 += 8 * bd) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + k * bd;
+            v[k] = i < m ? __ldg(src + i) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + k * bd;
+            if (i < m) dst[i] = v[k];
+        }
+    }
+}
+
+// Sums a dd over a worker: a warp, or the whole CTA (warp sums in warp
+// order through s_red).  The result is valid in the worker's thread 0.
+__device__ __forceinline__ dd worker_sum_dd(dd v, bool wide, dd* s_red)
+{
+    v = warp_sum_dd(v);
+    if (!wide) return v;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_red[wid] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) v = dd_add(v, s_red[i]);
+    return v;
+}
+
+__device__ __forceinline__ void worker_sync(bool wide)
+{
+    if (wide) __syncthreads();
+    else __syncwarp();
+}
+
+// A unit is refined by a worker: one warp per unit, or, when there are fewer
+// units than warps in the grid, one CTA per unit (the units then spread over
+// more SMs).  A worker's threads take terms; each runs two independent term
+// chains at a time when it has two.
+__global__ void __launch_bounds__(256) refine_real(Problem pb)
+{
+    const unsigned long long count = refine_count(pb);
     extern __shared__ __align__(16) double sm[];
+    __shared__ dd s_red[8];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const bool wide = count < (unsigned long long)gridDim.x * nwarps;
+    const int wk = wide ? blockDim.x : 32;               // threads per worker
+    const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
+    const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
     double* s_dh = sm;
     double* s_dl = s_dh + terms * n;
     double* s_x = s_dl + terms * n;      // [nwarps][2n]
     double* s_g = s_x + nwarps * 2 * n;  // [nwarps][nq]
-    for (int i = threadIdx.x; i < terms * n; i += blockDim.x) {
-        s_dh[i] = pb.de_hi[i];
-        s_dl[i] = pb.de_lo[i];
+    double* s_mt = s_g + nwarps * nq;    // [ntp][n]
+    // CTAs without a unit skip the tables (they still join the grid reduction)
+    if ((unsigned long long)blockIdx.x * nwk < count) {
+        stage(s_dh, pb.de_hi, terms * n);
+        stage(s_dl, pb.de_lo, terms * n);
+        stage(s_mt, pb.mt, ntp * n);
     }
     __syncthreads();
     double* xw = s_x + wid * 2 * n;
     double* gw = s_g + wid * nq;
     dd corr = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)blockIdx.x * nwarps + wid; e < count;
-         e += (unsigned long long)gridDim.x * nwarps) {
+    for (unsigned long long e = (unsigned long long)blockIdx.x * nwk + wid; e < count;
+         e += (unsigned long long)gridDim.x * nwk) {
         if (pb.list_x) {
             const double* src = pb.list_x + e * (2 * n);
-            for (int i = lane; i < 2 * n; i += 32) xw[i] = src[i];
+            for (int i = wl; i < 2 * n; i += wk) xw[i] = src[i];
         } else {
-            unit_base(pb, pb.list_u[e], 0, lane, xw, xw + n);
+            unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
         }
-        __syncwarp();
-        for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, pb.na, G);
+        worker_sync(wide);
+        for (int q = wl; q < nq; q += wk) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, pb.na, G);
         dd acc = {0.0, 0.0};
-        for (int d = lane; d < terms; d += 32) {
-            const int q = d / G, i = d % G;
-            int k = (q * n) * G + i;
-            dd p = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k], s_dl[k]});
-            for (int r = 1; r < n; ++r) {
-                k = (q * n + r) * G + i;
-                p = dd_mul(p, dd_add(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
+        if (terms >= 2 * wk) {
+            for (int d = wl; d < terms; d += 2 * wk) {
+                const int d2 = d + wk;
+                const int q1 = d / G, i1 = d % G, q2 = d2 / G, i2 = d2 % G;
+                int k1 = (q1 * n) * G + i1, k2 = (q2 * n) * G + i2;
+                dd p1 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k1], s_dl[k1]});
+                dd p2 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k2], s_dl[k2]});
+                for (int r = 1; r < n; ++r) {
+                    k1 = (q1 * n + r) * G + i1;
+                    k2 = (q2 * n + r) * G + i2;
+                    const dd x = {xw[r], xw[n + r]};
+                    p1 = dd_mul(p1, dd_add(x, dd{s_dh[k1], s_dl[k1]}));
+                    p2 = dd_mul(p2, dd_add(x, dd{s_dh[k2], s_dl[k2]}));
+                }
+                acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p1)) : dd_add(acc, p1);
+                acc = (__popc(d2) & 1) ? dd_add(acc, dd_neg(p2)) : dd_add(acc, p2);
             }
-            acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
+        } else {
+            for (int d = wl; d < terms; d += wk) {
+                const int q = d / G, i = d % G;
+                int k = (q * n) * G + i;
+                dd p = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k], s_dl[k]});
+                for (int r = 1; r < n; ++r) {
+                    k = (q * n + r) * G + i;
+                    p = dd_mul(p, dd_add(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
+                }
+                acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
+            }
         }
-        acc = warp_sum_dd(acc);
-        __syncwarp();
-        if (lane == 0) {
+        acc = worker_sum_dd(acc, wide, s_red);
+        worker_sync(wide);
+        if (wl == 0) {
             double f = 0.0;
             for (int q = 0; q < nq; ++q) f = (__popc(q) & 1) ? sub_rn(f, gw[q]) : add_rn(f, gw[q]);
             dd c = dd_add_d(acc, -f);
             if (pb.list_u[e] & 1ull) c = dd_neg(c);
             corr = dd_add(corr, c);
         }
-        __syncwarp();
+        worker_sync(wide);
     }
     dd tot[1] = {corr};
     grid_reduce<1>(tot, pb);
 }
 
-__global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long long count)
+__global__ void __launch_bounds__(256) refine_complex(Problem pb)
 {
+    const unsigned long long count = refine_count(pb);
     extern __shared__ __align__(16) double sm[];
+    __shared__ dd s_red[2][8];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const bool wide = count < (unsigned long long)gridDim.x * nwarps;
+    const int wk = wide ? blockDim.x : 32;               // threads per worker
+    const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
+    const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
     double* s_dh = sm;                    // [2][terms*n]
     double* s_dl = s_dh + 2 * terms * n;  // [2][terms*n]
     double* s_x = s_dl + 2 * terms * n;   // [nwarps][4n]
     double* s_g = s_x + nwarps * 4 * n;   // [nwarps][2*nq]
-    for (int i = threadIdx.x; i < 2 * terms * n; i += blockDim.x) {
-        s_dh[i] = pb.de_hi[i];
-        s_dl[i] = pb.de_lo[i];
+    double* s_mt = s_g + nwarps * 2 * nq; // [2][ntp][n]
+    // CTAs without a unit skip the tables (they still join the grid reduction)
+    if ((unsigned long long)blockIdx.x * nwk < count) {
+        stage(s_dh, pb.de_hi, 2 * terms * n);
+        stage(s_dl, pb.de_lo, 2 * terms * n);
+        stage(s_mt, pb.mt, 2 * ntp * n);
     }
     __syncthreads();
     const double* drh = s_dh;
@@ -298,21 +482,21 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
     double* xw = s_x + wid * 4 * n;  // xr hi, xr lo, xi hi, xi lo
     double* gw = s_g + wid * 2 * nq;
     dd corr_r = {0.0, 0.0}, corr_i = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)blockIdx.x * nwarps + wid; e < count;
-         e += (unsigned long long)gridDim.x * nwarps) {
+    for (unsigned long long e = (unsigned long long)blockIdx.x * nwk + wid; e < count;
+         e += (unsigned long long)gridDim.x * nwk) {
         if (pb.list_x) {
             const double* src = pb.list_x + e * (4 * n);
-            for (int i = lane; i < 4 * n; i += 32) xw[i] = src[i];
+            for (int i = wl; i < 4 * n; i += wk) xw[i] = src[i];
         } else {
-            unit_base(pb, pb.list_u[e], 0, lane, xw, xw + n);
-            unit_base(pb, pb.list_u[e], 1, lane, xw + 2 * n, xw + 3 * n);
+            unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
+            unit_base(pb, s_mt, pb.list_u[e], 1, wl, xw + 2 * n, xw + 3 * n, wk);
         }
-        __syncwarp();
-        for (int q = lane; q < nq; q += 32)
+        worker_sync(wide);
+        for (int q = wl; q < nq; q += wk)
             group_sum_complex_rt(xw, xw + 2 * n, drh + q * n * G, dih + q * n * G, n, G, gw[2 * q],
                                  gw[2 * q + 1]);
         dd ar = {0.0, 0.0}, ai = {0.0, 0.0};
-        for (int d = lane; d < terms; d += 32) {
+        for (int d = wl; d < terms; d += wk) {
             const int q = d / G, i = d % G;
             int k = (q * n) * G + i;
             dd pr = dd_add(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
@@ -334,10 +518,10 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
                 ai = dd_add(ai, pi);
             }
         }
-        ar = warp_sum_dd(ar);
-        ai = warp_sum_dd(ai);
-        __syncwarp();
-        if (lane == 0) {
+        ar = worker_sum_dd(ar, wide, s_red[0]);
+        ai = worker_sum_dd(ai, wide, s_red[1]);
+        worker_sync(wide);
+        if (wl == 0) {
             double fr = 0.0, fi = 0.0;
             for (int q = 0; q < nq; ++q) {
                 if (__popc(q) & 1) {
@@ -356,7 +540,7 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb, unsigned long 
             corr_r = dd_add(corr_r, cr);
             corr_i = dd_add(corr_i, ci);
         }
-        __syncwarp();
+        worker_sync(wide);
     }
     dd tot[2] = {corr_r, corr_i};
     grid_reduce<2>(tot, pb);
@@ -394,16 +578,16 @@ int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s)
     return SPB_OK;
 }
 
-int launch_scan_parallel(const Problem& pb, cudaStream_t s)
+int launch_listing(const Problem& pb, cudaStream_t s)
 {
-    scan_parallel<<<pb.grid * 4, 128, 0, s>>>(pb);
+    list_units<<<pb.grid * 4, 128, 0, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }
 
-int launch_collect(const Problem& pb, cudaStream_t s)
+int launch_threshold(const Problem& pb, cudaStream_t s)
 {
-    collect_listed<<<(unsigned)((pb.raw_cap + 255) / 256), 256, 0, s>>>(pb);
+    dd_threshold<<<1, 32, 0, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }
@@ -412,26 +596,46 @@ size_t refine_smem_bytes(const Problem& pb, int threads)
 {
     const size_t terms = (size_t)1 << pb.w, n = pb.n, c = pb.comps, nq = terms / pb.g;
     const size_t nwarps = threads / 32;
-    return sizeof(double) * (2 * c * terms * n + nwarps * (2 * c * n + c * nq));
+    const size_t ntp = pb.n - 1 - pb.w > 0 ? pb.n - 1 - pb.w : 0;
+    return sizeof(double) * (2 * c * terms * n + nwarps * (2 * c * n + c * nq) + c * ntp * n);
 }
 
-int launch_refine(const Problem& pb, unsigned long long count, int blocks, cudaStream_t s)
+int launch_refine(const Problem& pb, int blocks, cudaStream_t s)
 {
     const int threads = 256;
     const size_t smem = refine_smem_bytes(pb, threads);
-    auto kern = pb.comps == 1 ? refine_real : refine_complex;
-    int dev = 0, optin = 0;
+    const int ck = pb.comps == 1 ? 0 : 1;
+    auto kern = ck == 0 ? refine_real : refine_complex;
+    // The shared-memory limit is raised once per device and kernel.
+    static std::mutex mu;
+    static int limit[64][2];
+    int dev = 0;
     SPB_CUDA_TRY(cudaGetDevice(&dev));
-    SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    cudaFuncAttributes fa{};
-    SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
-    if (smem + fa.sharedSizeBytes > (size_t)optin) {
+    int room = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= 64) {
+            spb_set_error("refine: device %d out of range", dev);
+            return SPB_ERR_INVALID;
+        }
+        if (limit[dev][ck] == 0) {
+            int optin = 0;
+            cudaFuncAttributes fa{};
+            SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+            SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              optin - (int)fa.sharedSizeBytes));
+            limit[dev][ck] = optin - (int)fa.sharedSizeBytes;
+        }
+        room = limit[dev][ck];
+    }
+    if (smem > (size_t)room) {
         spb_set_error("refine: n=%d needs %zu B shared memory", pb.n, smem);
         return SPB_ERR_INVALID;
     }
-    SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      optin - (int)fa.sharedSizeBytes));
-    kern<<<blocks, threads, smem, s>>>(pb, count);
+    Problem pr = pb;
+    pr.result = pb.rb->corr;
+    kern<<<blocks, threads, smem, s>>>(pr);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }
