@@ -42,13 +42,18 @@ namespace dense {
 // ------------------------------------------------------------ setup kernel --
 // One CTA builds every table the walk kernels read.  The matrix is staged in
 // shared memory (dynamic, n*n*comps doubles: setup_smem_bytes), so the table
-// builds below read it at shared-memory latency.
-__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
+// builds below read it at shared-memory latency.  With smem_tables the
+// subset-sum table is also built in shared memory (each level reads the
+// levels below it) and written out once at the end.
+__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int smem_tables)
 {
     const int n = pb.n, c = pb.comps, w = pb.w, G = pb.g;
     const int tid = threadIdx.x, bd = blockDim.x;
     __shared__ int s_exp[kMaxN];
-    extern __shared__ double s_as[];  // [n][n][c], row-scaled after step 1
+    extern __shared__ double s_as[];  // [n][n][c], row-scaled after step 1; then the table
+    const int terms = 1 << w;
+    double* dh = smem_tables ? s_as + n * n * c : pb.de_hi;  // [c][terms/G][n][G]
+    double* dl = smem_tables ? dh + (size_t)c * terms * n : pb.de_lo;
 
     for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
     __syncthreads();
@@ -87,14 +92,13 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
     //    the double-double sum of the selected columns added in ascending
     //    order.  Built level by level: with k the highest bit of d,
     //    DE[d] = DE[d - 2^k] + a_k, the same operations in the same order.
-    const int terms = 1 << w;
     auto de_pos = [&](int part, int d, int r) {
         return (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
     };
     for (int idx = tid; idx < n * c; idx += bd) {
         const size_t pos = de_pos(idx / n, 0, idx % n);
-        pb.de_hi[pos] = 0.0;
-        pb.de_lo[pos] = 0.0;
+        dh[pos] = 0.0;
+        dl[pos] = 0.0;
         if (pb.de32) pb.de32[pos] = 0.0f;
     }
     for (int k = 0; k < w; ++k) {
@@ -104,10 +108,10 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
             const int part = idx / (half * n), rem = idx % (half * n);
             const int d = half + rem / n, r = rem % n;
             const size_t from = de_pos(part, d - half, r);
-            const dd s = dd_add_d(dd{pb.de_hi[from], pb.de_lo[from]}, s_as[(r * n + k) * c + part]);
+            const dd s = dd_add_d(dd{dh[from], dl[from]}, s_as[(r * n + k) * c + part]);
             const size_t pos = de_pos(part, d, r);
-            pb.de_hi[pos] = s.hi;
-            pb.de_lo[pos] = s.lo;
+            dh[pos] = s.hi;
+            dl[pos] = s.lo;
             if (pb.de32) pb.de32[pos] = __double2float_rn(s.hi);
         }
     }
@@ -117,7 +121,12 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
     //     bit patterns of non-negative doubles order like the values.
     __shared__ unsigned long long s_bmax[kMaxN];
     for (int r = tid; r < n; r += bd) s_bmax[r] = 0ull;
-    __syncthreads();  // the complex bound reads the table written above
+    __syncthreads();  // the complex bound and the write-out read the table written above
+    if (smem_tables)
+        for (int i = tid; i < c * terms * n; i += bd) {
+            pb.de_hi[i] = dh[i];
+            pb.de_lo[i] = dl[i];
+        }
     if (c == 1) {
         for (int r = tid; r < n; r += bd) {
             double lo = 0.0, hi = 0.0;
@@ -132,7 +141,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in)
         for (int idx = tid; idx < terms * n; idx += bd) {
             const int r = idx % n, d = idx / n;
             const size_t pos = ((size_t)(d / G) * n + r) * G + (d % G);
-            const double m = hypot(pb.de_hi[pos], pb.de_hi[(size_t)terms * n + pos]);
+            const double m = hypot(dh[pos], dh[(size_t)terms * n + pos]);
             atomicMax(&s_bmax[r], (unsigned long long)__double_as_longlong(m));
         }
         __syncthreads();
@@ -162,20 +171,30 @@ size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * 
 
 int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s)
 {
-    // up to 63*63*2 doubles (63.5 KB) of staged matrix: raise the dynamic limit once per device
+    // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits,
+    // the subset-sum table: raise the dynamic limit to the maximum once per device.
     static std::mutex mu;
-    static bool done[64] = {false};
+    static int room[64] = {0};
     int dev = 0;
     SPB_CUDA_TRY(cudaGetDevice(&dev));
+    int limit = 0;
     {
         std::lock_guard<std::mutex> lk(mu);
-        if (!done[dev & 63]) {
+        if (room[dev & 63] == 0) {
+            int optin = 0;
+            cudaFuncAttributes fa{};
+            SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, setup_kernel));
             SPB_CUDA_TRY(cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)setup_smem_bytes(kMaxN, 2)));
-            done[dev & 63] = true;
+                                              optin - (int)fa.sharedSizeBytes));
+            room[dev & 63] = optin - (int)fa.sharedSizeBytes;
         }
+        limit = room[dev & 63];
     }
-    setup_kernel<<<1, 512, setup_smem_bytes(pb.n, pb.comps), s>>>(pb, d_a);
+    const size_t base = setup_smem_bytes(pb.n, pb.comps);
+    const size_t tables = sizeof(double) * 2 * (size_t)pb.comps * ((size_t)1 << pb.w) * pb.n;
+    const int smem_tables = base + tables <= (size_t)limit ? 1 : 0;
+    setup_kernel<<<1, 512, base + (smem_tables ? tables : 0), s>>>(pb, d_a, smem_tables);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }

@@ -37,7 +37,7 @@
 namespace spb {
 namespace dense {
 // Defined in dense.cu.
-__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in);
+__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int smem_tables);
 int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s);
 int group_size(int n, int comps);
 int choose_unit_bits(int n, int comps, const spb_options* opt);
