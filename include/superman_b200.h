@@ -279,8 +279,8 @@ SPB_API int spb_decompose(const double* a, int n, int* count, int* sizes, double
  * reference, which computes one matrix per process run).  Requests are
  * admitted while the device memory they would occupy fits the budget, small
  * ones (n <= batch_max_n) are packed per (n, real/complex) into batched
- * launches (one warp per matrix, each batch shape captured once in a CUDA
- * graph and replayed), large ones run the whole-GPU walk on a second stream,
+ * launches (one warp per matrix; a batch shape used a few times is captured
+ * once in a CUDA graph and replayed), large ones run the whole-GPU walk on a second stream,
  * so both kinds overlap on the device.  A request's result does not depend on
  * what it was batched with. */
 typedef struct spb_server_config {

@@ -3,9 +3,11 @@
 //   submit ─► admission (queued bytes <= budget) ─► per-(n, real/complex) queue
 //      small (n <= batch_max_n):  batch worker packs up to max_batch requests of
 //        one shape into a free slot: host copy into the slot's pinned buffer,
-//        then one CUDA graph per (shape, padded count, slot) replays
-//        H2D copy -> batch_walk (one warp per matrix) -> D2H copy on the small
-//        stream; completion is detected with an event per slot, so up to
+//        then H2D copy -> batch_walk (one warp per matrix) -> D2H copy on the
+//        small stream, replayed from one CUDA graph per (shape, padded count,
+//        slot) once that key has been used kGraphAfterUses times (a capture
+//        costs far more than the plain launches of a rarely used key);
+//        completion is detected with an event per slot, so up to
 //        `slots` batches are in flight while new requests keep arriving.
 //      large: the large worker runs the whole-GPU walk on the library stream,
 //        concurrently with the batches.
@@ -56,6 +58,9 @@ struct Slot {
     std::vector<uint64_t> ids;
 };
 
+// Uses of a (shape, padded count, slot) key before its graph is captured.
+constexpr int kGraphAfterUses = 3;
+
 struct GraphKey {
     int n, comps, bucket, slot;
     bool operator<(const GraphKey& o) const
@@ -88,6 +93,7 @@ private:
     cudaStream_t small_stream = nullptr;
     std::vector<Slot> slots;
     std::map<GraphKey, cudaGraphExec_t> graphs;
+    std::map<GraphKey, int> key_uses;  // plain launches per key not yet captured
 
     std::mutex mu;
     std::condition_variable cv_work, cv_large, cv_done;
@@ -338,18 +344,16 @@ int Server::launch_slot(int si, int n, int comps, std::vector<uint64_t>& ids)
                                      cudaMemcpyDeviceToHost, small_stream));
         return SPB_OK;
     };
-    if (graphs_on) {
-        const GraphKey key{n, comps, bucket, si};
-        auto it = graphs.find(key);
+    const GraphKey key{n, comps, bucket, si};
+    auto it = graphs_on ? graphs.find(key) : graphs.end();
+    const bool replay = graphs_on && (it != graphs.end() || ++key_uses[key] >= kGraphAfterUses);
+    if (replay) {
         if (it == graphs.end()) {
-            // one plain launch of this shape first (sets kernel attributes
-            // outside any capture), then capture the copy-kernel-copy chain
-            int rc = spb_perm_batch_dev(s.d_in, n, comps == 2, 1, s.d_out, small_stream);
-            if (rc != SPB_OK) return rc;
-            SPB_CUDA_TRY(cudaStreamSynchronize(small_stream));
+            // The key's earlier plain launches set the kernel's attributes
+            // outside any capture; capture the copy-kernel-copy chain.
             cudaGraph_t g = nullptr;
             SPB_CUDA_TRY(cudaStreamBeginCapture(small_stream, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue();
+            int rc = enqueue();
             cudaError_t ce = cudaStreamEndCapture(small_stream, &g);
             if (rc != SPB_OK) return rc;
             SPB_CUDA_TRY(ce);
