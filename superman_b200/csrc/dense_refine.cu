@@ -214,18 +214,37 @@ __global__ void __launch_bounds__(128) list_units(Problem pb)
 }
 
 // *list_bin = the lowest bin whose tail (units at or above it) holds
-// at most raw_cap/2 units by bound_walk's count.
-__global__ void pick_list_bin(Problem pb)
+// at most raw_cap/2 units by bound_walk's count.  One warp; lane l owns bins
+// [16l, 16l + 16) and the tails are lane-local sums joined by a warp scan.
+__global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
 {
-    __shared__ unsigned s_c[kHistBins];
-    for (int i = threadIdx.x; i < kHistBins; i += blockDim.x) s_c[i] = pb.pre_cnt[i];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long tail = 0;
-        int b = kHistBins;
-        while (b > 0 && tail + s_c[b - 1] <= pb.raw_cap / 2) tail += s_c[--b];
-        *pb.list_bin = b;
+    constexpr int kPer = kHistBins / 32;
+    const int lane = threadIdx.x;
+    const unsigned full = 0xffffffffu;
+    unsigned long long cn[kPer], cl = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        cn[i] = pb.pre_cnt[lane * kPer + i];
+        cl += cn[i];
     }
+    unsigned long long sfx = cl;  // inclusive suffix over lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long p = __shfl_down_sync(full, sfx, d);
+        if (lane + d < 32) sfx += p;
+    }
+    unsigned long long tail = __shfl_down_sync(full, sfx, 1);
+    if (lane == 31) tail = 0;
+    const unsigned long long half = pb.raw_cap / 2;
+    int b = kHistBins;
+#pragma unroll
+    for (int i = kPer - 1; i >= 0; --i) {
+        tail += cn[i];
+        if (tail <= half) b = lane * kPer + i;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) b = min(b, __shfl_xor_sync(full, b, d));
+    if (lane == 0) *pb.list_bin = b;
 }
 
 // Picks the refinement bin: the lowest bin b such that the units below it,
@@ -315,12 +334,17 @@ __global__ void __launch_bounds__(32) dd_threshold(Problem pb)
         rb->err = mag > 0.0 ? sqrt(below) / mag : INFINITY;
         rb->from_list = (bsel >= *pb.list_bin && *pb.raw_n <= pb.raw_cap) ? 1 : 0;
         rb->list_n = 0;
+        // the refinement writes its correction only when it has units
+        rb->corr[0] = dd{0.0, 0.0};
+        rb->corr[1] = dd{0.0, 0.0};
     }
 }
 
 // Units to refine: the histogram's count when the listing found exactly
 // that many and the list held them all, else none (the host then lists
-// again and reruns the refinement).
+// again and reruns the refinement).  With none, the refine kernels return at
+// once (the count is the same for every CTA) and rb->corr keeps the zero
+// dd_threshold wrote.
 __device__ __forceinline__ unsigned long long refine_count(const Problem& pb)
 {
     const unsigned long long want = pb.rb->count;
@@ -374,6 +398,7 @@ __device__ __forceinline__ void worker_sync(bool wide)
 __global__ void __launch_bounds__(256) refine_real(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
+    if (count == 0) return;
     extern __shared__ __align__(16) double sm[];
     __shared__ dd s_red[8];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
@@ -455,6 +480,7 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb)
 __global__ void __launch_bounds__(256) refine_complex(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
+    if (count == 0) return;
     extern __shared__ __align__(16) double sm[];
     __shared__ dd s_red[2][8];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
@@ -573,7 +599,7 @@ int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s)
         return SPB_ERR_INVALID;
     }
     if (st != SPB_OK) return st;
-    pick_list_bin<<<1, 128, 0, s>>>(pb);
+    pick_list_bin<<<1, 32, 0, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }
