@@ -18,11 +18,20 @@
 namespace spb {
 namespace dense {
 
+// Column stride of the high columns in shared memory: a multiple of 4 floats
+// (16-byte rows, so row runs load as 16-byte vectors) whose quarter is odd,
+// so that lanes reading different columns j (each thread steps its own Gray
+// unit) at the same row fall in different 16-byte bank groups for j mod 8.
+__host__ __device__ constexpr int bound_col_stride(int n)
+{
+    return (((n + 3) & ~3) >> 2) & 1 ? ((n + 3) & ~3) : ((n + 3) & ~3) + 4;
+}
+
 // Shared memory: high columns and bound terms as floats, then the counts.
 __host__ __device__ inline size_t bound_smem_bytes_f(int n, int c, int w)
 {
     const int ntp = n - 1 - w > 0 ? n - 1 - w : 0;
-    return sizeof(float) * ((size_t)c * ntp * n + 2 * n) + sizeof(unsigned) * kHistBins;
+    return sizeof(float) * ((size_t)c * ntp * bound_col_stride(n) + 2 * n) + sizeof(unsigned) * kHistBins;
 }
 
 // Moves the binary exponent of p (normal, positive) into e; p keeps [1, 2).
@@ -37,12 +46,13 @@ template <int N, int C>
 __global__ void __launch_bounds__(256) bound_walk(Problem pb)
 {
     extern __shared__ __align__(16) float fsm[];
+    constexpr int S = bound_col_stride(N);
     const int ntop = N - 1 - pb.w, ntp = ntop > 0 ? ntop : 0;
     const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31;
-    float* s_mt = fsm;                   // [C][ntop][N]
-    float* s_b = s_mt + C * ntp * N;     // real [2][N] (mid, half), complex [N] (max |DE|)
+    float* s_mt = fsm;                   // [C][ntop][S], rows 0..N-1 used
+    float* s_b = s_mt + C * ntp * S;     // real [2][N] (mid, half), complex [N] (max |DE|)
     unsigned* s_cnt = reinterpret_cast<unsigned*>(s_b + 2 * N);
-    for (int i = tid; i < C * ntp * N; i += bd) s_mt[i] = (float)pb.mt[i];
+    for (int i = tid; i < C * ntp * N; i += bd) s_mt[(i / N) * S + i % N] = (float)pb.mt[i];
     for (int r = tid; r < N; r += bd) {
         if constexpr (C == 1) {
             s_b[r] = (float)(0.5 * (pb.bnd[r] + pb.bnd[N + r]));
@@ -69,7 +79,7 @@ __global__ void __launch_bounds__(256) bound_walk(Problem pb)
 #pragma unroll
         for (int c = 0; c < C; ++c)
 #pragma unroll
-            for (int r = 0; r < N; ++r) x[c][r] += s_mt[(c * ntp + j) * N + r];
+            for (int r = 0; r < N; ++r) x[c][r] += s_mt[(c * ntp + j) * S + r];
     }
 #pragma unroll
     for (int r = 0; r < N; ++r) hb[r] = C == 1 ? s_b[N + r] : s_b[r];
@@ -80,7 +90,7 @@ __global__ void __launch_bounds__(256) bound_walk(Problem pb)
 #pragma unroll
             for (int c = 0; c < C; ++c)
 #pragma unroll
-                for (int r = 0; r < N; ++r) x[c][r] = fmaf(sg, s_mt[(c * ntp + j) * N + r], x[c][r]);
+                for (int r = 0; r < N; ++r) x[c][r] = fmaf(sg, s_mt[(c * ntp + j) * S + r], x[c][r]);
         }
         float p = 1.0f;
         int e = 0;
