@@ -31,8 +31,10 @@ namespace {
 
 // One group of G terms, bitwise identical to unit_sum_real<N,G>'s group
 // (na == n) or to unit_sum_sparse<NA>'s (na < n: the inactive rows' product
-// first, then the na active rows; see sparse_impl.cuh).
-__device__ __forceinline__ double group_sum_real_rt(const double* xh, const double* de, int n, int na, int G)
+// first, then the na active rows; see sparse_impl.cuh).  The group's term i
+// of row r is de[r * rs + i].
+__device__ __forceinline__ double group_sum_real_rt(const double* xh, const double* de, int n, int na, int G,
+                                                    int rs)
 {
     double p0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
     p0 = add_rn(xh[0], de[0]);
@@ -51,11 +53,11 @@ __device__ __forceinline__ double group_sum_real_rt(const double* xh, const doub
     }
     for (int r = 1; r < na; ++r) {
         const double x = xh[r];
-        p0 = mul_rn(p0, add_rn(x, de[r * G + 0]));
-        if (G >= 2) p1 = mul_rn(p1, add_rn(x, de[r * G + 1]));
+        p0 = mul_rn(p0, add_rn(x, de[r * rs + 0]));
+        if (G >= 2) p1 = mul_rn(p1, add_rn(x, de[r * rs + 1]));
         if (G == 4) {
-            p2 = mul_rn(p2, add_rn(x, de[r * G + 2]));
-            p3 = mul_rn(p3, add_rn(x, de[r * G + 3]));
+            p2 = mul_rn(p2, add_rn(x, de[r * rs + 2]));
+            p3 = mul_rn(p3, add_rn(x, de[r * rs + 3]));
         }
     }
     if (G == 4) return sub_rn(sub_rn(p0, p1), sub_rn(p2, p3));
@@ -64,9 +66,10 @@ __device__ __forceinline__ double group_sum_real_rt(const double* xh, const doub
 }
 
 // One group of G (<= 4) complex terms, bitwise identical to unit_sum_complex<N,G>.
+// The group's term i of row r is dr/di[r * rs + i].
 __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const double* xi,
                                                      const double* dr, const double* di, int n,
-                                                     int G, double& gr, double& gi)
+                                                     int G, int rs, double& gr, double& gi)
 {
     double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = 0; i < G; ++i) {
@@ -75,8 +78,8 @@ __device__ __forceinline__ void group_sum_complex_rt(const double* xr, const dou
     }
     for (int r = 1; r < n; ++r) {
         for (int i = 0; i < G; ++i) {
-            double yr = add_rn(xr[r], dr[r * G + i]);
-            double yi = add_rn(xi[r], di[r * G + i]);
+            double yr = add_rn(xr[r], dr[r * rs + i]);
+            double yi = add_rn(xi[r], di[r * rs + i]);
             double t1 = mul_rn(pi[i], yi);
             double t2 = mul_rn(pi[i], yr);
             double nr = __fma_rn(pr[i], yr, -t1);
@@ -371,6 +374,33 @@ __device__ __forceinline__ void stage(double* dst, const double* __restrict__ sr
     }
 }
 
+// Copies `parts` subset-sum tables laid out [q][n][G] (the walks' grouping,
+// q = d / G) into shared memory as [n][terms] (d contiguous per row), so
+// that lanes taking consecutive terms of one row read consecutive words
+// rather than words n*G apart in one bank.  Eight loads in flight per thread.
+__device__ __forceinline__ void stage_rows(double* dst, const double* __restrict__ src, int parts, int n,
+                                           int terms, int G)
+{
+    const int per = terms * n, m = parts * per, bd = blockDim.x;
+    for (int i0 = threadIdx.x; i0 < m; i0 += 8 * bd) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + k * bd;
+            v[k] = i < m ? __ldg(src + i) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + k * bd;
+            if (i < m) {
+                const int part = i / per, rem = i % per;
+                const int q = rem / (n * G), rg = rem % (n * G);
+                dst[part * per + (rg / G) * terms + q * G + rg % G] = v[k];
+            }
+        }
+    }
+}
+
 // Sums a dd over a worker: a warp, or the whole CTA (warp sums in warp
 // order through s_red).  The result is valid in the worker's thread 0.
 __device__ __forceinline__ dd worker_sum_dd(dd v, bool wide, dd* s_red)
@@ -391,19 +421,19 @@ __device__ __forceinline__ void worker_sync(bool wide)
     else __syncwarp();
 }
 
-// A unit is refined by a worker: one warp per unit, or, when there are fewer
-// units than warps in the grid, one CTA per unit (the units then spread over
+// A unit is refined by a worker: one warp per unit, or, when there are at
+// most as many units as CTAs, one CTA per unit (the units then spread over
 // more SMs).  A worker's threads take terms; each runs two independent term
 // chains at a time when it has two.
-__global__ void __launch_bounds__(256) refine_real(Problem pb)
+__global__ void __launch_bounds__(512) refine_real(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
     if (count == 0) return;
     extern __shared__ __align__(16) double sm[];
-    __shared__ dd s_red[8];
+    __shared__ dd s_red[16];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
     const int nwarps = blockDim.x >> 5;
-    const bool wide = count < (unsigned long long)gridDim.x * nwarps;
+    const bool wide = count <= (unsigned long long)gridDim.x;  // one unit per CTA at most
     const int wk = wide ? blockDim.x : 32;               // threads per worker
     const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
     const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
@@ -414,8 +444,8 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb)
     double* s_mt = s_g + nwarps * nq;    // [ntp][n]
     // CTAs without a unit skip the tables (they still join the grid reduction)
     if ((unsigned long long)blockIdx.x * nwk < count) {
-        stage(s_dh, pb.de_hi, terms * n);
-        stage(s_dl, pb.de_lo, terms * n);
+        stage_rows(s_dh, pb.de_hi, 1, n, terms, G);  // [n][terms]
+        stage_rows(s_dl, pb.de_lo, 1, n, terms, G);
         stage(s_mt, pb.mt, ntp * n);
     }
     __syncthreads();
@@ -431,18 +461,15 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb)
             unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
         }
         worker_sync(wide);
-        for (int q = wl; q < nq; q += wk) gw[q] = group_sum_real_rt(xw, s_dh + q * n * G, n, pb.na, G);
+        for (int q = wl; q < nq; q += wk) gw[q] = group_sum_real_rt(xw, s_dh + q * G, n, pb.na, G, terms);
         dd acc = {0.0, 0.0};
         if (terms >= 2 * wk) {
             for (int d = wl; d < terms; d += 2 * wk) {
                 const int d2 = d + wk;
-                const int q1 = d / G, i1 = d % G, q2 = d2 / G, i2 = d2 % G;
-                int k1 = (q1 * n) * G + i1, k2 = (q2 * n) * G + i2;
-                dd p1 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k1], s_dl[k1]});
-                dd p2 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k2], s_dl[k2]});
+                dd p1 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
+                dd p2 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
                 for (int r = 1; r < n; ++r) {
-                    k1 = (q1 * n + r) * G + i1;
-                    k2 = (q2 * n + r) * G + i2;
+                    const int k1 = r * terms + d, k2 = r * terms + d2;
                     const dd x = {xw[r], xw[n + r]};
                     p1 = dd_mul(p1, dd_add(x, dd{s_dh[k1], s_dl[k1]}));
                     p2 = dd_mul(p2, dd_add(x, dd{s_dh[k2], s_dl[k2]}));
@@ -452,11 +479,9 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb)
             }
         } else {
             for (int d = wl; d < terms; d += wk) {
-                const int q = d / G, i = d % G;
-                int k = (q * n) * G + i;
-                dd p = dd_add(dd{xw[0], xw[n]}, dd{s_dh[k], s_dl[k]});
+                dd p = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
                 for (int r = 1; r < n; ++r) {
-                    k = (q * n + r) * G + i;
+                    const int k = r * terms + d;
                     p = dd_mul(p, dd_add(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
                 }
                 acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
@@ -477,15 +502,15 @@ __global__ void __launch_bounds__(256) refine_real(Problem pb)
     grid_reduce<1>(tot, pb);
 }
 
-__global__ void __launch_bounds__(256) refine_complex(Problem pb)
+__global__ void __launch_bounds__(512) refine_complex(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
     if (count == 0) return;
     extern __shared__ __align__(16) double sm[];
-    __shared__ dd s_red[2][8];
+    __shared__ dd s_red[2][16];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
     const int nwarps = blockDim.x >> 5;
-    const bool wide = count < (unsigned long long)gridDim.x * nwarps;
+    const bool wide = count <= (unsigned long long)gridDim.x;  // one unit per CTA at most
     const int wk = wide ? blockDim.x : 32;               // threads per worker
     const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
     const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
@@ -496,8 +521,8 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb)
     double* s_mt = s_g + nwarps * 2 * nq; // [2][ntp][n]
     // CTAs without a unit skip the tables (they still join the grid reduction)
     if ((unsigned long long)blockIdx.x * nwk < count) {
-        stage(s_dh, pb.de_hi, 2 * terms * n);
-        stage(s_dl, pb.de_lo, 2 * terms * n);
+        stage_rows(s_dh, pb.de_hi, 2, n, terms, G);  // [2][n][terms]
+        stage_rows(s_dl, pb.de_lo, 2, n, terms, G);
         stage(s_mt, pb.mt, 2 * ntp * n);
     }
     __syncthreads();
@@ -519,16 +544,15 @@ __global__ void __launch_bounds__(256) refine_complex(Problem pb)
         }
         worker_sync(wide);
         for (int q = wl; q < nq; q += wk)
-            group_sum_complex_rt(xw, xw + 2 * n, drh + q * n * G, dih + q * n * G, n, G, gw[2 * q],
+            group_sum_complex_rt(xw, xw + 2 * n, drh + q * G, dih + q * G, n, G, terms, gw[2 * q],
                                  gw[2 * q + 1]);
         dd ar = {0.0, 0.0}, ai = {0.0, 0.0};
         for (int d = wl; d < terms; d += wk) {
-            const int q = d / G, i = d % G;
-            int k = (q * n) * G + i;
+            int k = d;
             dd pr = dd_add(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
             dd pi = dd_add(dd{xw[2 * n], xw[3 * n]}, dd{dih[k], dil[k]});
             for (int r = 1; r < n; ++r) {
-                k = (q * n + r) * G + i;
+                k = r * terms + d;
                 dd yr = dd_add(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
                 dd yi = dd_add(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
                 dd nr = dd_add(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
@@ -628,8 +652,10 @@ size_t refine_smem_bytes(const Problem& pb, int threads)
 
 int launch_refine(const Problem& pb, int blocks, cudaStream_t s)
 {
-    const int threads = 256;
-    const size_t smem = refine_smem_bytes(pb, threads);
+    // 512 threads (16 warps per SM hide the double-double latency chains)
+    // when their per-warp buffers fit next to the tables, else 256.
+    int threads = 512;
+    size_t smem = refine_smem_bytes(pb, threads);
     const int ck = pb.comps == 1 ? 0 : 1;
     auto kern = ck == 0 ? refine_real : refine_complex;
     // The shared-memory limit is raised once per device and kernel.
@@ -654,6 +680,10 @@ int launch_refine(const Problem& pb, int blocks, cudaStream_t s)
             limit[dev][ck] = optin - (int)fa.sharedSizeBytes;
         }
         room = limit[dev][ck];
+    }
+    if (smem > (size_t)room) {
+        threads = 256;
+        smem = refine_smem_bytes(pb, threads);
     }
     if (smem > (size_t)room) {
         spb_set_error("refine: n=%d needs %zu B shared memory", pb.n, smem);
