@@ -328,13 +328,26 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
         // (the refinement's rebuild does the same).  Row by row: with the
         // column loop outermost the compiler keeps every row's lo word live
         // and the walk spills.
+        // Four rows at a time: independent add chains (the same operations
+        // per row, in the same order).
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-            dd x = {pb.x0_hi[r], pb.x0_lo[r]};
+        for (int r0 = 0; r0 < N; r0 += 4) {
+            dd x[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (r0 + k < N) x[k] = dd{pb.x0_hi[r0 + k], pb.x0_lo[r0 + k]};
             for (int j = 0; j < ntop; ++j)
-                if ((g0 >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
-            xh[r] = x.hi;
-            s_lo[r * bd + tid] = x.lo;
+                if ((g0 >> j) & 1ull) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (r0 + k < N) x[k] = dd_add_d(x[k], s_mt[j * N + r0 + k]);
+                }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (r0 + k < N) {
+                    xh[r0 + k] = x[k].hi;
+                    s_lo[(r0 + k) * bd + tid] = x[k].lo;
+                }
         }
         unsigned long long u = u0;
         while (true) {
@@ -506,19 +519,33 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
     if (u0 < u1) {
         double xr[N], xi[N];
         const unsigned long long g0 = gray_of(u0);
+        // Two rows (four add chains) at a time, the same operations per row.
 #pragma unroll
-        for (int r = 0; r < N; ++r) {
-            dd a = {pb.x0_hi[r], pb.x0_lo[r]};
-            dd b = {pb.x0_hi[N + r], pb.x0_lo[N + r]};
+        for (int r0 = 0; r0 < N; r0 += 2) {
+            dd a[2], b[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                if (r0 + k < N) {
+                    a[k] = dd{pb.x0_hi[r0 + k], pb.x0_lo[r0 + k]};
+                    b[k] = dd{pb.x0_hi[N + r0 + k], pb.x0_lo[N + r0 + k]};
+                }
             for (int j = 0; j < ntop; ++j)
                 if ((g0 >> j) & 1ull) {
-                    a = dd_add_d(a, s_mt_re[j * N + r]);
-                    b = dd_add_d(b, s_mt_im[j * N + r]);
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+                        if (r0 + k < N) {
+                            a[k] = dd_add_d(a[k], s_mt_re[j * N + r0 + k]);
+                            b[k] = dd_add_d(b[k], s_mt_im[j * N + r0 + k]);
+                        }
                 }
-            xr[r] = a.hi;
-            xi[r] = b.hi;
-            s_lo_re[r * bd + tid] = a.lo;
-            s_lo_im[r * bd + tid] = b.lo;
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                if (r0 + k < N) {
+                    xr[r0 + k] = a[k].hi;
+                    xi[r0 + k] = b[k].hi;
+                    s_lo_re[(r0 + k) * bd + tid] = a[k].lo;
+                    s_lo_im[(r0 + k) * bd + tid] = b[k].lo;
+                }
         }
         unsigned long long u = u0;
         while (true) {

@@ -56,16 +56,34 @@ __global__ void __launch_bounds__(F32Cfg<N, C>::kMaxThreads, 1) walk_f32(Problem
     if (u0 < u1) {
         double xh[C][N];
         const unsigned long long g0 = gray_of(u0);
+        // R rows of every part (four add chains) at a time, the same
+        // operations per row.
+        constexpr int R = 4 / C;
 #pragma unroll
-        for (int c = 0; c < C; ++c)
+        for (int r0 = 0; r0 < N; r0 += R) {
+            dd x[C][R];
 #pragma unroll
-            for (int r = 0; r < N; ++r) {
-                dd x = {pb.x0_hi[c * N + r], pb.x0_lo[c * N + r]};
-                for (int j = 0; j < ntop; ++j)
-                    if ((g0 >> j) & 1ull) x = dd_add_d(x, s_mt[(c * ntp + j) * N + r]);
-                xh[c][r] = x.hi;
-                s_lo[(c * N + r) * bd + tid] = x.lo;
-            }
+            for (int c = 0; c < C; ++c)
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+                    if (r0 + k < N) x[c][k] = dd{pb.x0_hi[c * N + r0 + k], pb.x0_lo[c * N + r0 + k]};
+            for (int j = 0; j < ntop; ++j)
+                if ((g0 >> j) & 1ull) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c)
+#pragma unroll
+                        for (int k = 0; k < R; ++k)
+                            if (r0 + k < N) x[c][k] = dd_add_d(x[c][k], s_mt[(c * ntp + j) * N + r0 + k]);
+                }
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+#pragma unroll
+                for (int k = 0; k < R; ++k)
+                    if (r0 + k < N) {
+                        xh[c][r0 + k] = x[c][k].hi;
+                        s_lo[(c * N + r0 + k) * bd + tid] = x[c][k].lo;
+                    }
+        }
         unsigned long long u = u0;
         while (true) {
             float xf[C][N];

@@ -133,13 +133,25 @@ __global__ void __launch_bounds__(512, 1) walk_sparse(Problem pb)
         const unsigned long long g0 = gray_of(u0);
         // First unit base: x0 plus the selected high columns in index order,
         // zeros included (the same operations as the refinement's rebuild).
+        // Four rows at a time: independent add chains, the same operations per row.
 #pragma unroll
-        for (int r = 0; r < NA; ++r) {
-            dd x = {pb.x0_hi[r], pb.x0_lo[r]};
+        for (int r0 = 0; r0 < NA; r0 += 4) {
+            dd x[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (r0 + k < NA) x[k] = dd{pb.x0_hi[r0 + k], pb.x0_lo[r0 + k]};
             for (int j = 0; j < ntop; ++j)
-                if ((g0 >> j) & 1ull) x = dd_add_d(x, s_ma[j * NA + r]);
-            xa[r] = x.hi;
-            s_lo[r * bd + tid] = x.lo;
+                if ((g0 >> j) & 1ull) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (r0 + k < NA) x[k] = dd_add_d(x[k], s_ma[j * NA + r0 + k]);
+                }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (r0 + k < NA) {
+                    xa[r0 + k] = x[k].hi;
+                    s_lo[(r0 + k) * bd + tid] = x[k].lo;
+                }
         }
         for (int k = 0; k < ni; ++k) {
             dd x = {pb.x0_hi[NA + k], pb.x0_lo[NA + k]};
