@@ -56,6 +56,19 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
     double* dl = smem_tables ? dh + (size_t)c * terms * n : pb.de_lo;
 
     for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
+    // 0. What the later kernels of the call accumulate into starts at zero.
+    if (tid < 4) pb.ticket[tid] = 0u;
+    if (pb.mode != 0) {
+        for (int i = tid; i < kHistBins; i += bd) {
+            pb.hist_s2[i] = 0.0;
+            pb.hist_cnt[i] = 0ull;
+            pb.pre_cnt[i] = 0u;
+        }
+        if (tid == 0) {
+            *pb.raw_n = 0ull;
+            *pb.list_bin = pb.list_bin_init;
+        }
+    }
     __syncthreads();
     // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in [0.5, 1).
     for (int r = tid; r < n; r += bd) {
@@ -398,29 +411,23 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
                                      cudaMemcpyHostToDevice, stream));
         d_a = d_in;
     }
-    SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
-    if (dd_mode) {
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_s2, 0, sizeof(double) * kHistBins, stream));
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.hist_cnt, 0, sizeof(unsigned long long) * kHistBins, stream));
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.pre_cnt, 0, sizeof(unsigned) * kHistBins, stream));
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.raw_n, 0, sizeof(unsigned long long), stream));
-    }
+    // The walk's list bin, written by the setup kernel (which also zeroes the
+    // counters and histograms): 0 lists every unit when all fit the list;
+    // 0x7f7f7f7f, above every bin, lists none (the row-compacted walk, whose
+    // refinement goes through the scan); with a bound pass pick_list_bin
+    // overwrites it.
+    pb.list_bin_init = (pb.na == n && pb.units <= pb.raw_cap / 2) ? 0 : 0x7f7f7f7f;
     if ((st = launch_setup(pb, d_a, stream)) != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaGetLastError());
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
     int launches = 2;
-    if (dd_mode && pb.na == n && pb.units <= pb.raw_cap / 2) {
-        // every unit fits the list: list them all (bin 0 and up), no bound pass
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.list_bin, 0, sizeof(int), stream));
-    } else if (dd_mode && pb.na == n) {
+    if (dd_mode && pb.na == n && pb.units > pb.raw_cap / 2) {
         // Size the first pass's unit list from a bound-only pass (about 1.5 %
         // of a dense walk).  The row-compacted walk has few terms per unit, so
         // there the pass would cost a large share; it lists nothing and a
         // refinement, when one is needed, goes through the scan.
         if ((st = launch_bound_pass(pb, blocks, stream)) != SPB_OK) return out->status = st;
         launches += 2;
-    } else if (dd_mode) {  // 0x7f7f7f7f: above every bin
-        SPB_CUDA_TRY(cudaMemsetAsync(pb.list_bin, 0x7f, sizeof(int), stream));
     }
     st = pb.f32 ? launch_walk_f32(pb, blocks, threads, smem, stream) : launch_walk(pb, blocks, threads, smem, stream);
     if (st != SPB_OK) return out->status = st;

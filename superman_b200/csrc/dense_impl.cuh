@@ -63,6 +63,7 @@ struct Problem {
     // raw_cap, and the walk appends every unit at or above it (raw_*).
     unsigned* pre_cnt;             // [kHistBins]
     int* list_bin;
+    int list_bin_init;             // written to *list_bin by setup_kernel (pick_list_bin may overwrite it)
     unsigned long long* raw_n;
     unsigned long long raw_cap;
     unsigned long long* raw_u;     // [raw_cap] unit index
