@@ -182,28 +182,34 @@ namespace dense {
 
 size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
 
-int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s)
+// The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
+// subset-sum table: the setup kernel's dynamic shared-memory limit is raised to
+// the maximum once per device (which also loads the kernel); *limit receives it.
+int prepare_setup(int* limit)
 {
-    // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits,
-    // the subset-sum table: raise the dynamic limit to the maximum once per device.
     static std::mutex mu;
     static int room[64] = {0};
     int dev = 0;
     SPB_CUDA_TRY(cudaGetDevice(&dev));
-    int limit = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (room[dev & 63] == 0) {
-            int optin = 0;
-            cudaFuncAttributes fa{};
-            SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, setup_kernel));
-            SPB_CUDA_TRY(cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              optin - (int)fa.sharedSizeBytes));
-            room[dev & 63] = optin - (int)fa.sharedSizeBytes;
-        }
-        limit = room[dev & 63];
+    std::lock_guard<std::mutex> lk(mu);
+    if (room[dev & 63] == 0) {
+        int optin = 0;
+        cudaFuncAttributes fa{};
+        SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, setup_kernel));
+        SPB_CUDA_TRY(cudaFuncSetAttribute(setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          optin - (int)fa.sharedSizeBytes));
+        room[dev & 63] = optin - (int)fa.sharedSizeBytes;
     }
+    if (limit) *limit = room[dev & 63];
+    return SPB_OK;
+}
+
+int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s)
+{
+    int limit = 0;
+    int st = prepare_setup(&limit);
+    if (st != SPB_OK) return st;
     const size_t base = setup_smem_bytes(pb.n, pb.comps);
     const size_t tables = sizeof(double) * 2 * (size_t)pb.comps * ((size_t)1 << pb.w) * pb.n;
     const int smem_tables = base + tables <= (size_t)limit ? 1 : 0;

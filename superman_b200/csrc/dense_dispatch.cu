@@ -30,6 +30,15 @@ int launch_walk_complex(const Problem& pb, int blocks, int threads, size_t smem,
     }
 }
 
+int prepare_walk_real(int n)
+{
+    Problem pb{};
+    pb.n = n;
+    pb.na = n;
+    pb.comps = 1;
+    return launch_walk_real(pb, 0, 0, 0, nullptr);  // blocks = 0: load and configure, no launch
+}
+
 int walk_max_threads(int n, int comps)
 {
     return comps == 1 ? RealMaxThreads(n) : ComplexMaxThreads(n);

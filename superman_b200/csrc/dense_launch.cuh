@@ -34,6 +34,7 @@ int launch_complex_n(const Problem& pb, int blocks, int threads, size_t smem, cu
                     optin - (int)fa.sharedSizeBytes);                                           \
         });                                                                                     \
         SPB_CUDA_TRY(attr_err[dev & 63]);                                                       \
+        if (blocks <= 0) return SPB_OK; /* prepare only: kernel loaded, attributes set */       \
         KERNEL<N><<<blocks, threads, smem, s>>>(pb);                                            \
         SPB_CUDA_TRY(cudaGetLastError());                                                       \
         return SPB_OK;                                                                          \

@@ -8,6 +8,10 @@ allocation failure.  The variant keeps its working memory in one fixed device
 array inside the library, so each call here passes only device input and
 output buffers (allocated by the caller, torch in this test).
 
+Both entry points run the FP64 walk with the same launch shape, so their
+results agree to the tolerance of the other dense parity tests (in practice
+bit for bit), at every size the fixed array takes, 40 included.
+
 This file is collected last on purpose: it runs after every other GPU test in
 a full run, and it also passes alone in a fresh process.
 """
@@ -30,7 +34,7 @@ def _call(L, d_a, n, d_out):
                                         ctypes.c_void_p(d_out.data_ptr()), None)
 
 
-@pytest.mark.parametrize("n", [1, 5, 20, 28, 32])
+@pytest.mark.parametrize("n", [1, 5, 20, 28, 32, 36, 40])
 def test_noalloc_matches_allocating_entry_twice(spb, n):
     import torch
     L = _lib.lib()
@@ -48,6 +52,33 @@ def test_noalloc_matches_allocating_entry_twice(spb, n):
         hi, lo = d_out.cpu().numpy()
         assert abs(hi - want) <= REL_TOL * abs(want), (hi, want)
         assert abs(lo) <= abs(hi) * 2.0 ** -52
+
+
+def test_noalloc_calls_allocate_nothing(spb):
+    """With every library allocation set to fail, the calls still succeed, and
+    the device's free memory does not move across them (the set-up, which
+    loads the kernels, happened in a first call)."""
+    import torch
+    L = _lib.lib()
+    sizes = [12, 24, 33, 40]
+    mats = [torch.from_numpy(W.dense_uniform(n, seed=950 + n)).cuda() for n in sizes]
+    outs = [torch.zeros(2, dtype=torch.float64, device="cuda") for _ in sizes]
+    _lib.check(_call(L, mats[0], sizes[0], outs[0]))  # set-up on this device
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    L.spb_debug_fail_allocations(1 << 30)
+    try:
+        sts = [_call(L, d_a, n, d_out) for d_a, n, d_out in zip(mats, sizes, outs)]
+        torch.cuda.synchronize()
+    finally:
+        L.spb_debug_fail_allocations(0)
+    free1, _ = torch.cuda.mem_get_info()
+    assert sts == [_lib.SPB_OK] * len(sizes), sts
+    assert free1 == free0, (free0, free1)
+    for n, d_out in zip(sizes, outs):
+        hi = float(d_out[0])
+        want = spb.perm_dense(W.dense_uniform(n, seed=950 + n)).permanent
+        assert abs(hi - want) <= REL_TOL * abs(want), (n, hi, want)
 
 
 def test_noalloc_rejects_sizes_beyond_its_array(spb):
