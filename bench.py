@@ -12,8 +12,9 @@ exchange; one process per GPU, max-over-ranks device time).
 
 Printed JSON line (rank 0):
   value      device-resident input, CUDA-event time per step on the launch stream
-  e2e        same metric through the C ABI with a pinned host matrix: H2D copy,
-             kernels, D2H of the result inside the timed region
+  e2e        same metric through the C ABI with a pinned host matrix, timed by
+             the host clock around each call: H2D copy, kernels, D2H of the
+             result and the call's host work inside the timed region
   roofline   dominant kernel (the Gray walk): FP64 pipe instructions per
              launch / walk-kernel time, against the FP64 FMA pipe peak measured
              by a DFMA microbenchmark in the same run
@@ -51,7 +52,7 @@ WORKLOADS = {
 }
 
 # DRAM bytes (read + write) per walk_real<32> launch, from one ncu capture of
-# this workload (profiles/traffic_walk_real_n32.md).
+# this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {"dense32": 199424}
 
 
@@ -333,8 +334,12 @@ def ours_arm(args, wl):
         return res.device_s, res.kernel_s, res.launches
 
     def step_host():
+        # host wall clock around the public C-ABI call on the pinned host
+        # matrix: H2D copy, kernels, D2H of the result and the call's own
+        # host work (the call returns after its stream synchronize)
+        t0 = time.perf_counter()
         _lib.check(fn_host(host_ptr, n, ctypes.byref(opt), ctypes.byref(res)))
-        return res.device_s, res.kernel_s, res.launches
+        return time.perf_counter() - t0, res.kernel_s, res.launches
 
     def timed(step):
         for _ in range(args.warmup):
@@ -428,7 +433,8 @@ def ours_arm(args, wl):
                        "precision": args.precision, "l2": "flushed between steps (256 MiB write)",
                        "permanent": repr(value_dev), "rel_err_vs_exact": err},
             "e2e": {"value": e2e, "unit": "gray-steps/s", "h2d_bytes_per_step": n * n * 8 * comps,
-                    "d2h_bytes_per_step": 16 * comps + 4},
+                    "d2h_bytes_per_step": 16 * comps + 4,
+                    "timing": "host wall clock (perf_counter) around each spb_perm_dense_* call"},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
             "gpu_launches": launches}
     if f32 is not None:

@@ -205,12 +205,18 @@ SPB_API int spb_perm_binary(const uint8_t* a, int n, const spb_options* opt, uin
  * for their own pool allocator, and latency-bound request loops that cannot
  * take cudaFree's device-wide synchronisation or an allocation failure
  * mid-request.  d_a: device, n*n doubles row-major; d_out: device, 2 doubles
- * receiving the permanent as a double-double (hi, lo).  Runs asynchronously
- * on `stream` (NULL = the default stream); read d_out after synchronising.
- * Working memory is one fixed 256 KiB device array per GPU inside the
- * library, so n is limited to 1..40 (larger n: SPB_ERR_INVALID).  The first
- * call on a device looks up that array's address (make it before any stream
- * capture).  All calls share the array: calls that overlap on the GPU race.
+ * receiving the permanent as (hi, lo).  Runs asynchronously on `stream`
+ * (NULL = the default stream); read d_out after synchronising.
+ * Precision is that of SPB_PREC_FP64 (FP64 row sums and products,
+ * double-double sums, no double-double refinement): about 1e-13 relative at
+ * n=24 and 3e-12 at n=32 on U[0,1) entries, so lo is not a double-double
+ * accurate correction.  Working memory is one fixed 256 KiB device array per
+ * GPU inside the library, so n is limited to 1..40 (larger n:
+ * SPB_ERR_INVALID).  The first call on a device looks up that array's address
+ * and loads the kernels the call can launch (CUDA loads modules lazily by
+ * default, which can allocate): make it before reserving the rest of device
+ * memory for a pool, and before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race.
  * No counterpart in the reference, which allocates on every call
  * (Algorithms/GPU/Dense/dpSingleGPU.cuh:138-144). */
 SPB_API int spb_perm_dense_f64_noalloc(const double* d_a, int n, double* d_out, void* stream);
@@ -258,6 +264,21 @@ SPB_API int spb_read_matrix(const char* path, int binary, int undirected, int is
  * *has_perfect_matching (0: the permanent is structurally zero and out is
  * all zeros).  Replaces dm() (IO/dm.cpp:441-501).  CPU only. */
 SPB_API int spb_dm_prune(const double* a, int n, double* out, int* has_perfect_matching);
+
+/* The pieces main.cpp's real-matrix flow (main.cpp:63-110) computes for a
+ * matrix, without computing them: perfect-matching pruning (IO/IO.h:477-508),
+ * connected components (IO/dm.h:43-107) and DecomposePerman
+ * (CommonFiles/DecomposePerman.h:76-557) on each component, with the default
+ * settings.  The permanent of the matrix is the product over the
+ * *components of the sum of the permanents of each component's pieces (a
+ * component without pieces contributes 0: a structurally zero permanent is
+ * one component with no pieces).  *count pieces; sizes[k], piece_component[k]
+ * and the row-major entries concatenated in data.  Pass sizes =
+ * piece_component = data = NULL to query *components and *count alone.
+ * The reference prints the piece count and their mean size as "Submatrix
+ * count" and "Average N" (main.cpp:117-121).  CPU only. */
+SPB_API int spb_plan_pieces(const double* a, int n, int* components, int* count, int* sizes,
+                            int* piece_component, double* data, int max_pieces, size_t max_doubles);
 
 /* The reference's row/column orderings (IO/IO.h:598-1112) applied to a
  * row-major n x n matrix: order is "colSort", "rowSort" (param 0 ascending,

@@ -332,6 +332,24 @@ def ref_binary_path() -> str:
     return _REF_BIN
 
 
+def run_reference_stats(mtx_path: str, threads=None, extra=(), timeout=3600) -> dict:
+    """Like run_reference, plus the decomposition line the reference prints
+    (main.cpp:117-121): {"permanent", "seconds", "pieces", "avg_n", "avg_nnz"}."""
+    import re
+    import tempfile
+    work = tempfile.mkdtemp(prefix="spb_ref_")
+    os.makedirs(os.path.join(work, "build"), exist_ok=True)
+    args = [_REF_BIN, "pid=2", f"repo_dir={work}/", f"filename={mtx_path}", "mode=cpu",
+            f"thread_count={_threads(threads)}", *extra]
+    out = subprocess.run(args, check=True, capture_output=True, text=True, timeout=timeout).stdout
+    m = re.search(r"Submatrix count: (\d+) - Average N: (\S+) - Average NNZ: (\S+)", out)
+    p = re.search(r"Permanent: (\S+) - Computed in: (\S+) seconds", out)
+    if m is None or p is None:
+        raise RuntimeError("unexpected reference output: " + out[-400:])
+    return {"permanent": float(p.group(1)), "seconds": float(p.group(2)), "pieces": int(m.group(1)),
+            "avg_n": float(m.group(2)), "avg_nnz": float(m.group(3))}
+
+
 def run_reference(mtx_path: str, threads=None, extra=(), timeout=3600):
     """Run the reference's own CPU program on a matrix file; returns
     (permanent as float or complex, seconds).  Needs oracle/_ref built.

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import SPB_PREC_DD, SPB_PREC_FP64, SupermanError
 
-__all__ = ["Result", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "perm_approx",
+__all__ = ["Result", "plan_pieces", "perm_dense", "perm_sparse", "perm_complex", "perm_binary", "perm_approx",
            "approx_samples", "SupermanError", "SPB_PREC_FP64", "SPB_PREC_DD", "device_count"]
 
 _PREC = {"fp64": SPB_PREC_FP64, "kahan": SPB_PREC_FP64, "dd": SPB_PREC_DD, "fp32": 2}
@@ -141,6 +141,35 @@ def approx_samples(a, first: int, count: int, seed: int = 1) -> np.ndarray:
     _lib.check(_lib.lib().spb_approx_samples(cptrs.ctypes.data_as(ip), rows.ctypes.data_as(ip), cptrs.size - 1,
                                              first, count, seed, est.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     return est
+
+
+def plan_pieces(a):
+    """The pieces the reference's real-matrix flow computes for `a` (pruning,
+    connected components, DecomposePerman per component), without computing
+    them: (components, [(component, piece matrix)]).  The permanent of `a` is
+    the product over components of the sum of their pieces' permanents; a
+    component without pieces contributes 0.  CPU only."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    comps, count = ctypes.c_int(), ctypes.c_int()
+    L = _lib.lib()
+    _lib.check(L.spb_plan_pieces(a.ctypes.data_as(dp), n, ctypes.byref(comps), ctypes.byref(count),
+                                 None, None, None, 0, 0))
+    k = count.value
+    sizes = np.zeros(max(k, 1), dtype=np.int32)
+    owner = np.zeros(max(k, 1), dtype=np.int32)
+    data = np.zeros(max(k * n * n, 1))
+    _lib.check(L.spb_plan_pieces(a.ctypes.data_as(dp), n, ctypes.byref(comps), ctypes.byref(count),
+                                 sizes.ctypes.data_as(ip), owner.ctypes.data_as(ip), data.ctypes.data_as(dp),
+                                 k, data.size))
+    out, off = [], 0
+    for i in range(k):
+        m = int(sizes[i])
+        out.append((int(owner[i]), data[off:off + m * m].reshape(m, m).copy()))
+        off += m * m
+    return comps.value, out
 
 
 def perm_binary(a, device: int = 0, **shape) -> Result:

@@ -154,6 +154,9 @@ SIGNATURES = {
     "spb_dm_prune": (ctypes.c_int, [_DP, ctypes.c_int, _DP, ctypes.POINTER(ctypes.c_int)]),
     "spb_decompose": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int), _DP, ctypes.c_int, ctypes.c_size_t]),
+    "spb_plan_pieces": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _DP,
+                                       ctypes.c_int, ctypes.c_size_t]),
     "spb_server_create": (ctypes.c_int, [ctypes.POINTER(spb_server_config), ctypes.POINTER(ctypes.c_void_p)]),
     "spb_server_submit": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_uint64)]),

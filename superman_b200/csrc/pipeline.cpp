@@ -8,6 +8,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -34,11 +35,12 @@ Settings settings_from(const char* const* args, int nargs)
     return s;
 }
 
-// main.cpp:63-110 on an in-memory matrix (the reader's pruning included).
-void real_pipeline(Matrix<double>* matrix, Settings& settings, spb_pipeline_result* out)
+// Entries on no perfect matching removed in place, as IO::readMatrix does
+// (IO/IO.h:477-508); the sparsity is updated.
+void prune_in_place(Matrix<double>* matrix)
 {
     const int n = matrix->nov;
-    {   // prune entries on no perfect matching, as IO::readMatrix does
+    {
         std::vector<int> rptrs(n + 1, 0), cols;
         for (int r = 0; r < n; ++r) {
             for (int c = 0; c < n; ++c)
@@ -52,6 +54,24 @@ void real_pipeline(Matrix<double>* matrix, Settings& settings, spb_pipeline_resu
         std::copy(kept.begin(), kept.end(), matrix->mat);
         matrix->sparsity = n ? 100.0 * rptrs[n] / ((double)n * n) : 0.0;
     }
+}
+
+// Component k of the pruned matrix as its own square block (main.cpp:91-101).
+void component_block(const Matrix<double>* matrix, const std::vector<unsigned>& rows,
+                     const std::vector<unsigned>& cols, Matrix<double>* block)
+{
+    const int n = matrix->nov;
+    const unsigned m = (unsigned)rows.size();
+    for (unsigned i = 0; i < m; ++i)
+        for (unsigned j = 0; j < m; ++j) block->mat[(size_t)i * m + j] = matrix->mat[(size_t)rows[i] * n + cols[j]];
+    block->sparsity = 100.0 * getNNZ(block) / ((double)m * m);
+}
+
+// main.cpp:63-110 on an in-memory matrix (the reader's pruning included).
+void real_pipeline(Matrix<double>* matrix, Settings& settings, spb_pipeline_result* out)
+{
+    const int n = matrix->nov;
+    prune_in_place(matrix);
     std::vector<std::vector<unsigned>> rc, cc;
     unsigned biggest = 0;
     findCCs(matrix, rc, cc, biggest);
@@ -63,11 +83,8 @@ void real_pipeline(Matrix<double>* matrix, Settings& settings, spb_pipeline_resu
             result.permanent = 0;
             break;
         }
-        const unsigned m = (unsigned)rc[k].size();
-        Matrix<double> block(m);
-        for (unsigned i = 0; i < m; ++i)
-            for (unsigned j = 0; j < m; ++j) block.mat[(size_t)i * m + j] = matrix->mat[(size_t)rc[k][i] * n + cc[k][j]];
-        block.sparsity = 100.0 * getNNZ(&block) / ((double)m * m);
+        Matrix<double> block((int)rc[k].size());
+        component_block(matrix, rc[k], cc[k], &block);
         Result b = algorithm(&block, &settings);
         result.time += b.time;
         result.permanent *= b.permanent;
@@ -214,6 +231,65 @@ extern "C" int spb_decompose(const double* a, int n, int* count, int* sizes, dou
         }
         for (auto* p : ps) delete p;
         return st;
+    });
+}
+
+extern "C" int spb_plan_pieces(const double* a, int n, int* components, int* count, int* sizes,
+                               int* piece_component, double* data, int max_pieces, size_t max_doubles)
+{
+    if (!a || !components || !count || n < 1) {
+        spb_set_error("spb_plan_pieces: null argument or n < 1");
+        return SPB_ERR_INVALID;
+    }
+    return guarded([&] {
+        Settings s;
+        Matrix<double> m(n);
+        std::copy(a, a + (size_t)n * n, m.mat);
+        prune_in_place(&m);
+        std::vector<std::vector<unsigned>> rc, cc;
+        unsigned biggest = 0;
+        findCCs(&m, rc, cc, biggest);
+        struct NoDriver : Permanent<double, double> {
+            NoDriver(Matrix<double>* x, Settings st) : Permanent<double, double>(x, st) {}
+            double permanentFunction() override { return 0.0; }
+        };
+        std::vector<std::unique_ptr<Matrix<double>>> ps;
+        std::vector<int> owner;
+        int ncomp = 0;
+        for (size_t k = 0; k < rc.size(); ++k) {
+            if (rc[k].size() != cc[k].size()) {  // structurally zero (main.cpp:86-90)
+                ps.clear();
+                owner.clear();
+                ncomp = 1;
+                break;
+            }
+            Matrix<double> block((int)rc[k].size());
+            component_block(&m, rc[k], cc[k], &block);
+            DecomposePerman<double, double, NoDriver> d(&block, s);
+            for (Matrix<double>* p : d.pieces()) {
+                ps.emplace_back(p);
+                owner.push_back(ncomp);
+            }
+            ++ncomp;
+        }
+        *components = ncomp;
+        *count = (int)ps.size();
+        size_t need = 0;
+        for (auto& p : ps) need += (size_t)p->nov * p->nov;
+        if (!sizes && !piece_component && !data) return (int)SPB_OK;
+        if (!sizes || !piece_component || !data || (int)ps.size() > max_pieces || need > max_doubles) {
+            spb_set_error("spb_plan_pieces: %d pieces of %zu doubles do not fit the arrays (%d, %zu)",
+                          (int)ps.size(), need, max_pieces, max_doubles);
+            return (int)SPB_ERR_INVALID;
+        }
+        size_t off = 0;
+        for (size_t k = 0; k < ps.size(); ++k) {
+            sizes[k] = ps[k]->nov;
+            piece_component[k] = owner[k];
+            std::memcpy(data + off, ps[k]->mat, sizeof(double) * (size_t)ps[k]->nov * ps[k]->nov);
+            off += (size_t)ps[k]->nov * ps[k]->nov;
+        }
+        return (int)SPB_OK;
     });
 }
 

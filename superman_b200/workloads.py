@@ -84,3 +84,63 @@ def haar_unitary(N: int, seed: int) -> np.ndarray:
 
 def haar_block(n: int, seed: int, N: int = 256) -> np.ndarray:
     return np.ascontiguousarray(haar_unitary(N, seed)[:n, :n])
+
+
+# ------------------------------------------------------------ serving stream --
+# Request i of the seeded serving stream: n uniform in [n_lo, n_hi]; with
+# probability 1/2 a real U[0, 1) matrix (dense_uniform(n, seed * 1000003 + i)),
+# else an n x n block, at seeded row/column offsets, of Haar unitary i % 4
+# (haar_unitary(256, seed + i % 4)).  One numpy Generator(seed) drives n, the
+# kind and the offsets, in that order per request.
+
+def serve_stream_meta(n_lo: int, n_hi: int, count: int, seed: int = 2026):
+    """[(n, is_complex, r0, c0)] per request, without building the matrices."""
+    rng = np.random.default_rng(seed)
+    meta = []
+    for _ in range(count):
+        n = int(rng.integers(n_lo, n_hi + 1))
+        if rng.random() < 0.5:
+            meta.append((n, False, 0, 0))
+        else:
+            r0, c0 = rng.integers(0, 256 - n + 1, size=2)
+            meta.append((n, True, int(r0), int(c0)))
+    return meta
+
+
+class ServeStream:
+    """Builds the matrices of the seeded serving stream on demand."""
+
+    def __init__(self, n_lo: int, n_hi: int, count: int, seed: int = 2026):
+        self.seed = seed
+        self.meta = serve_stream_meta(n_lo, n_hi, count, seed)
+        self._unitaries = {}
+
+    def __len__(self):
+        return len(self.meta)
+
+    def matrix(self, i: int) -> np.ndarray:
+        n, cplx, r0, c0 = self.meta[i]
+        if not cplx:
+            return dense_uniform(n, self.seed * 1000003 + i)
+        k = i % 4
+        if k not in self._unitaries:
+            self._unitaries[k] = haar_unitary(256, self.seed + k)
+        return np.ascontiguousarray(self._unitaries[k][r0:r0 + n, c0:c0 + n])
+
+    def matrices(self):
+        return [self.matrix(i) for i in range(len(self.meta))]
+
+    def first_index(self, n: int, cplx: bool) -> int:
+        """Index of the first request of size n and the given kind (-1 if none)."""
+        for i, (m, c, _, _) in enumerate(self.meta):
+            if m == n and c == cplx:
+                return i
+        return -1
+
+
+def matrix_sha256(a: np.ndarray) -> str:
+    """Digest of a matrix's float64 bytes (complex: interleaved re/im), row-major."""
+    import hashlib
+    a = np.ascontiguousarray(a)
+    b = a.view(np.float64) if np.iscomplexobj(a) else a.astype(np.float64, copy=False)
+    return hashlib.sha256(np.ascontiguousarray(b).tobytes()).hexdigest()

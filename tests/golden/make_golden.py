@@ -53,7 +53,9 @@ def write_mtx(path, a, complex_=False, binary=False):
         f.write("\n".join(rows) + "\n")
 
 
-def reference_run(a, threads, complex_=False, binary=False):
+def reference_run(a, threads, complex_=False, binary=False, stats=False):
+    """The reference program's output on `a`; with stats, also its
+    decomposition line (piece count, mean size and nonzeros)."""
     if not os.path.exists(O.ref_binary_path()):
         return None
     with tempfile.TemporaryDirectory() as d:
@@ -64,8 +66,14 @@ def reference_run(a, threads, complex_=False, binary=False):
             extra.append("complex=true")
         if binary:
             extra.append("binary=true")
-        val, secs = O.run_reference(p, threads=threads, extra=extra)
+        if stats:
+            st = O.run_reference_stats(p, threads=threads, extra=extra)
+            val, secs = st["permanent"], st["seconds"]
+        else:
+            val, secs = O.run_reference(p, threads=threads, extra=extra)
     out = {"threads": threads, "seconds": secs}
+    if stats:
+        out.update(pieces=st["pieces"], avg_n=st["avg_n"], avg_nnz=st["avg_nnz"])
     if complex_:
         out["value_re"] = repr(val.real)
         out["value_im"] = repr(val.imag)
@@ -115,7 +123,7 @@ def make(name, threads):
             fx["exact"] = frac_str(D.exact_perm_sparse(a))
         else:
             fx["exact"] = frac_str(O.exact_perm(a, threads=threads))
-        fx["reference"] = reference_run(a, threads)
+        fx["reference"] = reference_run(a, threads, stats=kind == "sparse")
     fx["oracle_seconds"] = time.time() - t0
     with open(os.path.join(HERE, name + ".json"), "w") as f:
         json.dump(fx, f, indent=0)
