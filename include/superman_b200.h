@@ -39,7 +39,9 @@ enum spb_status {
     SPB_ERR_CANCELLED = 7,  /* the request was cancelled                       */
     SPB_ERR_BUSY = 8,       /* admission refused: queue or scratch full        */
     SPB_ERR_IO = 9,         /* file could not be opened or parsed              */
-    SPB_ERR_NOT_SQUARE = 10 /* matrix file header is not square                */
+    SPB_ERR_NOT_SQUARE = 10,/* matrix file header is not square                */
+    SPB_ERR_ACCURACY = 11   /* SPB_PREC_FP32: the result (returned) has an
+                               estimated relative error above rel_tol          */
 };
 
 /* Precision modes.  SPB_PREC_FP64 corresponds to the reference's default
@@ -49,10 +51,13 @@ enum spb_precision {
     SPB_PREC_FP64 = 0, /* FP64 row sums and products, double-double sum      */
     SPB_PREC_DD = 1,   /* + double-double re-evaluation of dominant units    */
     SPB_PREC_FP32 = 2  /* FP32 row sums and products (double-double unit
-                          bases and sum), n <= 40: about twice the FP64
-                          rate, relative error of order kappa * n * 2^-24;
-                          for inputs where that is within the caller's
-                          bound                                            */
+                          bases and sum), 3 <= n <= 40: faster, relative
+                          error of order kappa * n * 2^-24.  The call
+                          estimates that error (out->err_est, from the sum
+                          of squared terms) and returns SPB_ERR_ACCURACY,
+                          with the result filled in, when it exceeds
+                          rel_tol (0 = 1e-12, which FP32 products never
+                          meet: pass the bound the caller accepts)        */
 };
 
 /* Walk used by spb_perm_sparse_f64. */
@@ -65,7 +70,8 @@ enum spb_sparse_walk {
 typedef struct spb_options {
     int device;            /* CUDA ordinal (Settings::deviceID)              */
     int precision;         /* enum spb_precision                             */
-    double rel_tol;        /* SPB_PREC_DD target relative error (0 = 1e-13)  */
+    double rel_tol;        /* SPB_PREC_DD target relative error (0 = 1e-13);
+                              SPB_PREC_FP32 accepted error (0 = 1e-12)      */
     int unit_bits;         /* log2 Gray terms per unit; 0 = automatic        */
     int threads_per_block; /* 0 = automatic                                  */
     int blocks;            /* 0 = automatic (persistent: one CTA per SM)     */
@@ -297,22 +303,33 @@ SPB_API int spb_decompose(const double* a, int n, int* count, int* sizes, double
 
 /* ------------------------------------------------------- serving ---- */
 /* A request loop for many permanents of mixed sizes (no counterpart in the
- * reference, which computes one matrix per process run).  Requests are
- * admitted while the device memory they would occupy fits the budget, small
- * ones (n <= batch_max_n) are packed per (n, real/complex) into batched
+ * reference, which computes one matrix per process run; the per-request
+ * semantics are those of the single-GPU drivers,
+ * Algorithms/GPU/Dense/dpSingleGPU.cuh:156-209).  A request is admitted
+ * while its matrix fits the server's device pool (admit_bytes of device
+ * memory, reserved from admission to completion); a real matrix with zero
+ * entries is pruned and decomposed on the host as the reference's main flow
+ * does (spb_plan_pieces), and its pieces run as independent requests.
+ * Small matrices (n <= 20) are packed per (n, real/complex) into batched
  * launches (one warp per matrix; a batch shape used a few times is captured
- * once in a CUDA graph and replayed), large ones run the whole-GPU walk on a second stream,
- * so both kinds overlap on the device.  A request's result does not depend on
- * what it was batched with. */
+ * once in a CUDA graph and replayed); mid-size ones (21 <= n <= batch_max_n)
+ * are batched when enough of one shape are queued and otherwise run like the
+ * large ones; large ones run the whole-GPU walk on large_workers streams with
+ * their own working memory, so batches and whole-GPU calls overlap on the
+ * device.  A request's result does not depend on what it was batched with. */
 typedef struct spb_server_config {
     int device;
-    int batch_max_n;      /* n <= this goes through batched launches (1..24; 0 = 20) */
-    int max_batch;        /* matrices per batched launch (0 = 2048)                 */
-    int slots;            /* batched launches in flight (0 = 4)                     */
-    double max_wait_s;    /* longest a small request waits for its batch to fill   */
-    size_t admit_bytes;   /* admission budget: queued matrices' bytes (0 = 256 MiB) */
-    int precision;        /* enum spb_precision for large requests                  */
+    int batch_max_n;      /* n <= this may go through batched launches (1..24; 0 = 24) */
+    int max_batch;        /* matrices per batched launch (0 = 2048)                     */
+    int slots;            /* batched launches in flight (0 = 4)                         */
+    double max_wait_s;    /* longest a small request waits for its batch to fill       */
+    size_t admit_bytes;   /* device pool for admitted matrices (0 = 256 MiB)            */
+    int precision;        /* enum spb_precision of whole-GPU requests (a zero-filled
+                             config gives SPB_PREC_FP64; spb_server_default_config and
+                             a NULL config give SPB_PREC_DD)                             */
     int use_graphs;       /* >= 0: replay captured batch shapes (default); < 0: plain launches */
+    int large_workers;    /* concurrent whole-GPU calls (0 = 2)                         */
+    int split;            /* >= 0: decompose real matrices with zeros (default); < 0: off */
 } spb_server_config;
 
 typedef struct spb_request_result {
@@ -325,12 +342,20 @@ typedef struct spb_request_result {
 typedef struct spb_server_stats {
     uint64_t submitted, completed, rejected, cancelled;
     uint64_t batches, batched_requests, graph_launches, graphs_captured, large_launches;
-    size_t queued_bytes;
+    size_t queued_bytes;          /* device pool bytes reserved by requests in the server */
+    uint64_t split_requests;      /* requests decomposed into pieces                       */
+    uint64_t pieces;              /* pieces they produced                                  */
+    uint64_t mid_to_large;        /* mid-size requests run as whole-GPU calls               */
+    size_t pool_bytes;            /* device pool size                                      */
 } spb_server_stats;
 
+/* Fills *cfg with the defaults (device 0, batch_max_n 24, 2048 per batch,
+ * 4 slots, 200 us fill window, 256 MiB pool, SPB_PREC_DD, graphs on, 2
+ * whole-GPU workers, decomposition on). */
+SPB_API void spb_server_default_config(spb_server_config* cfg);
 SPB_API int spb_server_create(const spb_server_config* cfg, void** server);
-/* Copies the row-major matrix (interleaved re/im when is_complex); SPB_ERR_BUSY
- * when admission refuses it. */
+/* Copies the row-major matrix (interleaved re/im when is_complex) into the
+ * server's pool; SPB_ERR_BUSY when admission refuses it (the pool is full). */
 SPB_API int spb_server_submit(void* server, const double* a, int n, int is_complex, uint64_t* ticket);
 /* Submits `count` matrices in one call (sizes ns[k], flags is_complex[k],
  * entries concatenated row-major in `mats`); tickets[k] receives each ticket,

@@ -25,6 +25,7 @@ SPB_ERR_CANCELLED = 7
 SPB_ERR_BUSY = 8
 SPB_ERR_IO = 9
 SPB_ERR_NOT_SQUARE = 10
+SPB_ERR_ACCURACY = 11
 
 # enum spb_precision
 SPB_PREC_FP64 = 0
@@ -96,6 +97,8 @@ class spb_server_config(ctypes.Structure):
         ("admit_bytes", ctypes.c_size_t),
         ("precision", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
+        ("large_workers", ctypes.c_int),
+        ("split", ctypes.c_int),
     ]
 
 
@@ -111,7 +114,9 @@ class spb_request_result(ctypes.Structure):
 class spb_server_stats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in (
         "submitted", "completed", "rejected", "cancelled", "batches", "batched_requests",
-        "graph_launches", "graphs_captured", "large_launches")] + [("queued_bytes", ctypes.c_size_t)]
+        "graph_launches", "graphs_captured", "large_launches")] + [("queued_bytes", ctypes.c_size_t)] + [
+        (k, ctypes.c_uint64) for k in ("split_requests", "pieces", "mid_to_large")] + [
+        ("pool_bytes", ctypes.c_size_t)]
 
 
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -157,6 +162,7 @@ SIGNATURES = {
     "spb_plan_pieces": (ctypes.c_int, [_DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _DP,
                                        ctypes.c_int, ctypes.c_size_t]),
+    "spb_server_default_config": (None, [ctypes.POINTER(spb_server_config)]),
     "spb_server_create": (ctypes.c_int, [ctypes.POINTER(spb_server_config), ctypes.POINTER(ctypes.c_void_p)]),
     "spb_server_submit": (ctypes.c_int, [ctypes.c_void_p, _DP, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_uint64)]),

@@ -16,13 +16,13 @@
 // decomposition path runs its independent pieces through it.
 #include <cuda_runtime.h>
 
+#include "batch.h"
 #include "dense_impl.cuh"
 #include "spb_common.cuh"
 
 namespace spb {
 namespace batch {
 
-constexpr int kMaxN = 24;
 constexpr int kWarpsPerCta = 4;
 
 template <int N, int C>
@@ -46,8 +46,17 @@ struct Cfg {
     static_assert(SMEM_DOUBLES % 4 == 0, "per-warp shared slice must keep 32-byte alignment");
 };
 
+// Matrix m of a batch starts at mats + m*N*N*C, or, with an offset table, at
+// mats + offs[m] * kOffsetUnit doubles (the serving loop's device pool).
+
+// With `src` (the serving loop's page-locked host mirror, mapped into the
+// device's address space, at the same offsets), each warp first copies its
+// matrix from src into its place in mats, so every matrix crosses the host
+// link once, in coalesced reads that overlap the other warps' work.
 template <int N, int C>
-__global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __restrict__ mats,
+__global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(double* __restrict__ mats,
+                                                                 const unsigned* __restrict__ offs,
+                                                                 const double* __restrict__ src,
                                                                  int count, double* __restrict__ out)
 {
     using Q = Cfg<N, C>;
@@ -63,7 +72,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
 
     const int total_warps = gridDim.x * kWarpsPerCta;
     for (int m = blockIdx.x * kWarpsPerCta + wid; m < count; m += total_warps) {
-        const double* A = mats + (size_t)m * N * N * C;
+        const size_t base = offs ? (size_t)offs[m] * kOffsetUnit : (size_t)m * N * N * C;
+        if (src) {
+            for (int i = lane; i < N * N * C; i += 32) mats[base + i] = src[base + i];
+            __syncwarp();  // orders the warp's writes before its reads below
+        }
+        const double* A = mats + base;
         // row exponents: row max scaled into [0.5, 1)
         for (int r = lane; r < N; r += 32) {
             double mx = 0.0;
@@ -168,7 +182,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) batch_walk(const double* __
 }
 
 template <int N, int C>
-int launch_n(const double* mats, int count, double* out, int sms, cudaStream_t s)
+int launch_n(double* mats, const unsigned* offs, const double* src, int count, double* out, int sms,
+             cudaStream_t s)
 {
     constexpr size_t smem = sizeof(double) * Cfg<N, C>::SMEM_DOUBLES * kWarpsPerCta;
     if (smem > 48 * 1024) {
@@ -180,9 +195,42 @@ int launch_n(const double* mats, int count, double* out, int sms, cudaStream_t s
     const int cap = sms * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    batch_walk<N, C><<<blocks, kWarpsPerCta * 32, smem, s>>>(mats, count, out);
+    batch_walk<N, C><<<blocks, kWarpsPerCta * 32, smem, s>>>(mats, offs, src, count, out);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
+}
+
+int dispatch(double* mats, const unsigned* offs, const double* src, int n, int is_complex, int count, double* out,
+             int sms, cudaStream_t s)
+{
+    const int key = n * 2 + (is_complex ? 1 : 0);
+    switch (key) {
+#define SPB_BCASE(N)                                                               \
+    case 2 * N: return launch_n<N, 1>(mats, offs, src, count, out, sms, s);        \
+    case 2 * N + 1: return launch_n<N, 2>(mats, offs, src, count, out, sms, s);
+        SPB_BCASE(1) SPB_BCASE(2) SPB_BCASE(3) SPB_BCASE(4) SPB_BCASE(5) SPB_BCASE(6) SPB_BCASE(7)
+        SPB_BCASE(8) SPB_BCASE(9) SPB_BCASE(10) SPB_BCASE(11) SPB_BCASE(12) SPB_BCASE(13)
+        SPB_BCASE(14) SPB_BCASE(15) SPB_BCASE(16) SPB_BCASE(17) SPB_BCASE(18) SPB_BCASE(19)
+        SPB_BCASE(20) SPB_BCASE(21) SPB_BCASE(22) SPB_BCASE(23) SPB_BCASE(24)
+#undef SPB_BCASE
+    default:
+        spb_set_error("batched walk: unsupported n=%d", n);
+        return SPB_ERR_INVALID;
+    }
+}
+
+int launch_gathered(const double* src, double* dst, const unsigned* d_offs, int n, int is_complex, int count,
+                    double* d_out, cudaStream_t s)
+{
+    if (n < 1 || n > kMaxN || count < 0) {
+        spb_set_error("batched walk: n=%d outside 1..%d or negative count", n, kMaxN);
+        return SPB_ERR_INVALID;
+    }
+    if (count == 0) return SPB_OK;
+    int dev = 0, sms = 0;
+    SPB_CUDA_TRY(cudaGetDevice(&dev));
+    SPB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return dispatch(dst, d_offs, src, n, is_complex, count, d_out, sms, s);
 }
 
 }  // namespace batch
@@ -205,18 +253,7 @@ extern "C" int spb_perm_batch_dev(const double* d_mats, int n, int is_complex, i
     SPB_CUDA_TRY(cudaGetDevice(&dev));
     SPB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int key = n * 2 + (is_complex ? 1 : 0);
-    switch (key) {
-#define SPB_BCASE(N)                                                    \
-    case 2 * N: return launch_n<N, 1>(d_mats, count, d_out, sms, s);    \
-    case 2 * N + 1: return launch_n<N, 2>(d_mats, count, d_out, sms, s);
-        SPB_BCASE(1) SPB_BCASE(2) SPB_BCASE(3) SPB_BCASE(4) SPB_BCASE(5) SPB_BCASE(6) SPB_BCASE(7)
-        SPB_BCASE(8) SPB_BCASE(9) SPB_BCASE(10) SPB_BCASE(11) SPB_BCASE(12) SPB_BCASE(13)
-        SPB_BCASE(14) SPB_BCASE(15) SPB_BCASE(16) SPB_BCASE(17) SPB_BCASE(18) SPB_BCASE(19)
-        SPB_BCASE(20) SPB_BCASE(21) SPB_BCASE(22) SPB_BCASE(23) SPB_BCASE(24)
-#undef SPB_BCASE
-    default:
-        spb_set_error("spb_perm_batch_dev: unsupported n=%d", n);
-        return SPB_ERR_INVALID;
-    }
+    // the matrices are read in place (the cast drops const: with no source
+    // the kernel only reads them)
+    return dispatch(const_cast<double*>(d_mats), nullptr, nullptr, n, is_complex, count, d_out, sms, s);
 }

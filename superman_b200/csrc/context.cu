@@ -39,6 +39,7 @@ extern "C" const char* spb_status_string(int status)
     case SPB_ERR_BUSY: return "busy";
     case SPB_ERR_IO: return "io error";
     case SPB_ERR_NOT_SQUARE: return "matrix is not square";
+    case SPB_ERR_ACCURACY: return "estimated error above the bound";
     default: return "unknown status";
     }
 }
@@ -82,6 +83,15 @@ DeviceContext* get_context(int device, int* st)
         *st = SPB_ERR_NO_DEVICE;
         return nullptr;
     }
+    std::unique_ptr<DeviceContext> ctx(create_context(device, st));
+    if (!ctx) return nullptr;
+    g_ctx[device] = std::move(ctx);
+    return g_ctx[device].get();
+}
+
+DeviceContext* create_context(int device, int* st)
+{
+    *st = SPB_OK;
     auto ctx = std::make_unique<DeviceContext>();
     ctx->device = device;
     cudaError_t e = cudaSetDevice(device);
@@ -98,13 +108,27 @@ DeviceContext* get_context(int device, int* st)
     if (e != cudaSuccess) {
         spb_set_error("device %d init failed: %s", device, cudaGetErrorString(e));
         *st = SPB_ERR_CUDA;
+        destroy_context(ctx.release());
         return nullptr;
     }
     // Dynamic shared memory budget for the walk kernels: the opt-in limit less
     // a reserve for their static shared arrays (reductions, flags).
     ctx->smem_optin = optin > 4096 ? (size_t)optin - 4096 : (size_t)optin;
-    g_ctx[device] = std::move(ctx);
-    return g_ctx[device].get();
+    return ctx.release();
+}
+
+void destroy_context(DeviceContext* ctx)
+{
+    if (!ctx) return;
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t ev : {ctx->ev_begin, ctx->ev_end, ctx->ev_call0, ctx->ev_call1, ctx->ev_ref0, ctx->ev_ref1})
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->list) cudaFree(ctx->list);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
 }
 
 // Allocation failures injected by spb_debug_fail_allocations: each of the

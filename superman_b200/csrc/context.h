@@ -31,6 +31,12 @@ struct DeviceContext {
 // Returns the context of `device`, creating it on first use (status in *st).
 DeviceContext* get_context(int device, int* st);
 
+// A context owned by the caller (not the device's shared one): its own
+// stream, events and arenas, so that calls through it can overlap calls
+// through other contexts on the same device.  Free with destroy_context.
+DeviceContext* create_context(int device, int* st);
+void destroy_context(DeviceContext* ctx);
+
 // Ensures ctx->scratch holds at least `bytes` (grows, never shrinks).
 int ensure_scratch(DeviceContext* ctx, size_t bytes);
 

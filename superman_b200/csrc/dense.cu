@@ -58,6 +58,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
     for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
     // 0. What the later kernels of the call accumulate into starts at zero.
     if (tid < 4) pb.ticket[tid] = 0u;
+    if (pb.f32 && tid == 0) pb.rb->err = 0.0;  // the FP32 walk's sum of squared terms
     if (pb.mode != 0) {
         for (int i = tid; i < kHistBins; i += bd) {
             pb.hist_s2[i] = 0.0;
@@ -319,7 +320,7 @@ size_t walk_smem_bytes(const Problem& pb, int threads)
 }
 
 int run(const double* a, bool a_on_device, int n, int comps, const spb_options* opt_in, spb_result* out,
-        const WalkPlan* plan)
+        const WalkPlan* plan, DeviceContext* own_ctx)
 {
     double t_start = wall_seconds();
     if (!out) {
@@ -334,7 +335,7 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         return out->status = SPB_ERR_INVALID;
     }
     int st = SPB_OK;
-    DeviceContext* ctx = get_context(opt.device, &st);
+    DeviceContext* ctx = own_ctx ? own_ctx : get_context(opt.device, &st);
     if (!ctx) return out->status = st;
     std::lock_guard<std::mutex> lk(ctx->mu);
     SPB_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -521,6 +522,26 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));
 
+    // FP32 products: estimated relative error of the result from the sum of
+    // squared terms s2 the walk accumulated.  A term carries k roundings of
+    // relative size up to 2^-24 (k = 2n real: n adds and n-1 multiplies; 4n
+    // complex), modelled as independent and uniform, so the error of the sum
+    // has standard deviation sqrt(s2 * k / 3) * 2^-24.
+    int f32_status = SPB_OK;
+    if (pb.f32) {
+        const double k = (comps == 1 ? 2.0 : 4.0) * n;
+        const double mag = comps == 1 ? std::fabs(res[0].hi) : std::hypot(res[0].hi, res[1].hi);
+        const double e = std::sqrt(hrb->err * k / 3.0) * 0x1p-24 / mag;
+        out->err_est = std::isfinite(e) ? e : HUGE_VAL;
+        const double bound = opt.rel_tol > 0.0 ? opt.rel_tol : kF32DefaultBound;
+        if (!(out->err_est <= bound)) {
+            spb_set_error("FP32 products: estimated relative error %.2e exceeds the bound %.2e (rel_tol); "
+                          "the result is returned but not within it: use SPB_PREC_FP64 or SPB_PREC_DD, "
+                          "or a looser rel_tol", out->err_est, bound);
+            f32_status = SPB_ERR_ACCURACY;
+        }
+    }
+
     // perm = (4(n%2)-2) * total * 2^E ; the factor is +-2, an exact power of two.
     const int e = exp_sum + 1;
     const double sgn = (n % 2) ? 1.0 : -1.0;
@@ -535,9 +556,9 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     out->gray_steps = (uint64_t)n << (n - 1);
     out->launches = launches;
     out->active_rows = pb.na;
-    out->status = SPB_OK;
+    out->status = f32_status;
     out->elapsed_s = wall_seconds() - t_start;
-    return SPB_OK;
+    return f32_status;
 }
 
 }  // namespace dense

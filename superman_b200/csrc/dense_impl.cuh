@@ -19,7 +19,8 @@ struct Readback {
     dd corr[2];                 // [comps] the refinement's correction
     unsigned long long list_n;  // units listed for the refinement
     unsigned long long count;   // units the histogram puts at or above thr
-    double err;                 // expected relative error of the unrefined units
+    double err;                 // SPB_PREC_DD: expected relative error of the unrefined units;
+                                // SPB_PREC_FP32: the walk's sum of squared terms
     int thr;                    // refinement bin
     int from_list;              // 1: the walk's own list holds every unit at or above thr
     int exp_sum;                // sum of the row scaling exponents
@@ -285,6 +286,73 @@ __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const dou
     return acc;
 }
 
+// First unit base of each thread, built cooperatively by its warp; every
+// lane of the warp calls this (it shuffles), whether it owns units or not.
+// The lanes' first units u0 lie in one range [ulo, uhi] (balanced_range is
+// monotonic in the thread index), so the Gray bits above P, the highest bit
+// where ulo and uhi differ, are the same for every lane.  Lane r adds the
+// high columns j > P selected by those common bits to x0_r (double-double,
+// ascending j) for rows r and r + 32, the warp broadcasts the N results,
+// and each lane adds its own columns j <= P (ascending), four rows at a time
+// (independent chains, the same operations per row).  Hi words go to xh,
+// lo words to the thread's shared slots s_lo[r * bd + tid].  Compared with
+// every lane adding all of its columns, this saves most of the double-double
+// adds when threads own few units (n <= 26).
+template <int N>
+__device__ __forceinline__ void first_base_real(const Problem& pb, const double* __restrict__ s_mt,
+                                                double* s_lo, int ntop, unsigned long long u0,
+                                                unsigned long long u1, int tid, int bd, double (&xh)[N])
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = tid & 31;
+    const unsigned act = __ballot_sync(full, u0 < u1);
+    if (act == 0u) return;  // warp-uniform
+    const int last = 31 - __clz(act);
+    const unsigned long long ulo = __shfl_sync(full, u0, 0), uhi = __shfl_sync(full, u0, last);
+    const int P = ulo == uhi ? -1 : 63 - __clzll(ulo ^ uhi);
+    const unsigned long long gc = gray_of(ulo);
+    dd c0 = {0.0, 0.0}, c1 = {0.0, 0.0};
+    if (lane < N) {
+        c0 = dd{pb.x0_hi[lane], pb.x0_lo[lane]};
+        if (N > 32 && lane + 32 < N) c1 = dd{pb.x0_hi[lane + 32], pb.x0_lo[lane + 32]};
+        for (int j = P + 1; j < ntop; ++j)
+            if ((gc >> j) & 1ull) {
+                c0 = dd_add_d(c0, s_mt[j * N + lane]);
+                if (N > 32 && lane + 32 < N) c1 = dd_add_d(c1, s_mt[j * N + lane + 32]);
+            }
+    }
+    const bool own = u0 < u1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+        const double h = __shfl_sync(full, r < 32 ? c0.hi : c1.hi, r & 31);
+        const double l = __shfl_sync(full, r < 32 ? c0.lo : c1.lo, r & 31);
+        xh[r] = h;
+        if (own) s_lo[r * bd + tid] = l;
+    }
+    if (!own) return;
+    const unsigned long long g0 = gray_of(u0);
+    const int jp = P + 1 < ntop ? P + 1 : ntop;  // private columns 0 .. jp-1
+#pragma unroll
+    for (int r0 = 0; r0 < N; r0 += 4) {
+        dd x[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (r0 + k < N) x[k] = dd{xh[r0 + k], s_lo[(r0 + k) * bd + tid]};
+        for (int j = 0; j < jp; ++j)
+            if ((g0 >> j) & 1ull) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (r0 + k < N) x[k] = dd_add_d(x[k], s_mt[j * N + r0 + k]);
+            }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (r0 + k < N) {
+                xh[r0 + k] = x[k].hi;
+                s_lo[(r0 + k) * bd + tid] = x[k].lo;
+            }
+    }
+}
+
 template <int N>
 __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem pb)
 {
@@ -322,34 +390,13 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     HistCache hc;
     const int lbin = mode == 1 ? __ldcg(pb.list_bin) : 0;
     int bmax = 0;
+    double xh[N];
+    // First unit base: x0 plus the selected high columns, the warp's common
+    // ones first (the refinement rebuilds bases in plain index order; the hi
+    // words agree unless a row value lies within ~2^-100 of a rounding
+    // midpoint, and then only that unit's correction carries one FP64 rounding).
+    first_base_real<N>(pb, s_mt, s_lo, ntop, u0, u1, tid, bd, xh);
     if (u0 < u1) {
-        double xh[N];
-        const unsigned long long g0 = gray_of(u0);
-        // First unit base: x0 plus the selected high columns in index order
-        // (the refinement's rebuild does the same).  Row by row: with the
-        // column loop outermost the compiler keeps every row's lo word live
-        // and the walk spills.
-        // Four rows at a time: independent add chains (the same operations
-        // per row, in the same order).
-#pragma unroll
-        for (int r0 = 0; r0 < N; r0 += 4) {
-            dd x[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (r0 + k < N) x[k] = dd{pb.x0_hi[r0 + k], pb.x0_lo[r0 + k]};
-            for (int j = 0; j < ntop; ++j)
-                if ((g0 >> j) & 1ull) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        if (r0 + k < N) x[k] = dd_add_d(x[k], s_mt[j * N + r0 + k]);
-                }
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (r0 + k < N) {
-                    xh[r0 + k] = x[k].hi;
-                    s_lo[(r0 + k) * bd + tid] = x[k].lo;
-                }
-        }
         unsigned long long u = u0;
         while (true) {
             int b = 0;
@@ -634,8 +681,11 @@ int launch_refine(const Problem& pb, int blocks, cudaStream_t s);
 int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s);
 int launch_listing(const Problem& pb, cudaStream_t s);
 
-// FP32-product walks (f32_impl.cuh), n <= kMaxF32N.
+// FP32-product walks (f32_impl.cuh), n <= kMaxF32N.  A result whose
+// estimated relative error exceeds opt.rel_tol (kF32DefaultBound when unset,
+// the library's accuracy bar) comes back with SPB_ERR_ACCURACY.
 constexpr int kMaxF32N = 40;
+constexpr double kF32DefaultBound = 1e-12;
 int launch_walk_f32(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
 size_t walk_f32_smem_bytes(const Problem& pb, int threads);
 int walk_f32_max_threads(int n, int comps);

@@ -11,6 +11,10 @@
 // as in the FP64 walk.  A term's relative error is of order n * 2^-24, so the
 // result's is of order kappa * n * 2^-24, with kappa = sqrt(sum t^2) / |sum t|.
 // That suits inputs whose kappa is small, e.g. Haar-random complex blocks.
+// The walk also sums every term's square (|t|^2 for complex) into
+// pb.rb->err (zeroed by setup_kernel), from which the host estimates the
+// result's relative error and refuses the result when it exceeds the
+// caller's bound.
 #pragma once
 
 #include "dense_impl.cuh"
@@ -53,6 +57,7 @@ __global__ void __launch_bounds__(F32Cfg<N, C>::kMaxThreads, 1) walk_f32(Problem
     dd tot[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) tot[c] = {0.0, 0.0};
+    double s2 = 0.0;  // sum of squared terms (the error estimate's input)
     if (u0 < u1) {
         double xh[C][N];
         const unsigned long long g0 = gray_of(u0);
@@ -121,6 +126,8 @@ __global__ void __launch_bounds__(F32Cfg<N, C>::kMaxThreads, 1) walk_f32(Problem
                         gsum[0] = (double)p[0] - (double)p[1];
                     else
                         gsum[0] = (double)p[0];
+#pragma unroll
+                    for (int i = 0; i < G; ++i) s2 = __fma_rn((double)p[i], (double)p[i], s2);
                 } else {
                     const float* dr = s_de + q * (N * G);
                     const float* di = s_de + terms * N + q * (N * G);
@@ -164,6 +171,9 @@ __global__ void __launch_bounds__(F32Cfg<N, C>::kMaxThreads, 1) walk_f32(Problem
                         gsum[0] = (double)pr[0];
                         gsum[1] = (double)pi[0];
                     }
+#pragma unroll
+                    for (int i = 0; i < G; ++i)
+                        s2 = __fma_rn((double)pi[i], (double)pi[i], __fma_rn((double)pr[i], (double)pr[i], s2));
                 }
 #pragma unroll
                 for (int c = 0; c < C; ++c) acc[c] = (__popc(q) & 1) ? acc[c] - gsum[c] : acc[c] + gsum[c];
@@ -185,6 +195,9 @@ __global__ void __launch_bounds__(F32Cfg<N, C>::kMaxThreads, 1) walk_f32(Problem
                 }
         }
     }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, m);
+    if ((tid & 31) == 0) atomicAdd(&pb.rb->err, s2);
     grid_reduce<C>(tot, pb);
 }
 

@@ -152,7 +152,7 @@ bool plan_compacted(const double* a, int n, int mode, const spb_options& opt, Ch
 
 }  // namespace
 
-int run_real_host(const double* a, int n, const spb_options* opt, spb_result* out)
+int run_real_host(const double* a, int n, const spb_options* opt, spb_result* out, DeviceContext* ctx)
 {
     if (a && n >= 1 && n <= kMaxN && opt->sparse_walk != SPB_SPARSE_WALK_NEVER) {
         bool has_zero = false;
@@ -163,10 +163,10 @@ int run_real_host(const double* a, int n, const spb_options* opt, spb_result* ou
             for (int i = 0; i < n; ++i)
                 for (int j = 0; j < n; ++j) ap[(size_t)i * n + j] = a[(size_t)ch.rows[i] * n + ch.cols[j]];
             WalkPlan plan{ch.na, ch.w};
-            return run(ap.data(), false, n, 1, opt, out, &plan);
+            return run(ap.data(), false, n, 1, opt, out, &plan, ctx);
         }
     }
-    return run(a, false, n, 1, opt, out, nullptr);
+    return run(a, false, n, 1, opt, out, nullptr, ctx);
 }
 
 }  // namespace dense

@@ -1,7 +1,8 @@
 """Python handle on the serving loop of libsupb200 (spb_server_* in
 include/superman_b200.h): submit permanents of mixed size and type, poll or
-wait for them; small ones are batched on the GPU, large ones run the
-whole-GPU walk, concurrently."""
+wait for them; admission by device pool memory, small ones batched on the
+GPU, large ones on the whole-GPU walk, concurrently; real matrices with
+zeros decomposed into independent pieces."""
 from __future__ import annotations
 
 import ctypes
@@ -11,13 +12,21 @@ import numpy as np
 from . import _lib
 
 
+_PREC = {"fp64": _lib.SPB_PREC_FP64, "dd": _lib.SPB_PREC_DD, "fp32": _lib.SPB_PREC_FP32}
+
+
 class Server:
-    def __init__(self, device=0, batch_max_n=20, max_batch=2048, slots=4, max_wait_s=200e-6,
-                 admit_bytes=256 << 20, precision="fp64", use_graphs=True):
+    """Defaults follow spb_server_default_config: whole-GPU requests in
+    double-double refinement mode (<= 1e-12 relative at n=32), a 256 MiB
+    device pool for admitted matrices, batched launches up to n=24, two
+    concurrent whole-GPU workers, real matrices with zeros decomposed."""
+
+    def __init__(self, device=0, batch_max_n=24, max_batch=2048, slots=4, max_wait_s=200e-6,
+                 admit_bytes=256 << 20, precision="dd", use_graphs=True, large_workers=2, split=True):
         cfg = _lib.spb_server_config(device=device, batch_max_n=batch_max_n, max_batch=max_batch, slots=slots,
-                                     max_wait_s=max_wait_s, admit_bytes=admit_bytes,
-                                     precision=_lib.SPB_PREC_DD if precision == "dd" else _lib.SPB_PREC_FP64,
-                                     use_graphs=0 if use_graphs else -1)
+                                     max_wait_s=max_wait_s, admit_bytes=admit_bytes, precision=_PREC[precision],
+                                     use_graphs=0 if use_graphs else -1, large_workers=large_workers,
+                                     split=0 if split else -1)
         self._h = ctypes.c_void_p()
         _lib.check(_lib.lib().spb_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
 
@@ -53,6 +62,24 @@ class Server:
         _lib.check(_lib.lib().spb_server_submit_many(self._h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                      n_arr, c_arr, k, t_arr, ctypes.byref(got)))
         return [t_arr[i] for i in range(k)]
+
+    def submit_flat(self, buf, ns, is_complex):
+        """Queues len(ns) matrices already packed one after another in the
+        float64 array `buf` (row-major, complex ones as interleaved re/im),
+        with sizes ns and flags is_complex (int32 arrays); returns their
+        tickets (0 where admission refused one).  No per-matrix Python work,
+        for clients that keep their requests packed."""
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        ns = np.ascontiguousarray(ns, dtype=np.int32)
+        cx = np.ascontiguousarray(is_complex, dtype=np.int32)
+        k = int(ns.size)
+        t_arr = (ctypes.c_uint64 * max(1, k))()
+        got = ctypes.c_int()
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.check(_lib.lib().spb_server_submit_many(self._h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                     ns.ctypes.data_as(ip), cx.ctypes.data_as(ip), k, t_arr,
+                                                     ctypes.byref(got)))
+        return list(t_arr[:k])
 
     def poll(self, ticket):
         """The request's result dict when done, else None."""
