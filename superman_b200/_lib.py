@@ -52,6 +52,7 @@ class spb_options(ctypes.Structure):
         ("stream", ctypes.c_void_p),
         ("sparse_walk", ctypes.c_int),
         ("replay_listing", ctypes.c_int),
+        ("small_call", ctypes.c_int),
     ]
 
 

@@ -183,6 +183,11 @@ namespace dense {
 
 size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
 
+// The fused small-matrix call (small_call.cu).
+constexpr int kSmallCallMaxN = 24;
+size_t small_call_smem_bytes(int n, int w, int threads);
+int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, cudaStream_t s, bool* launched);
+
 // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
 // subset-sum table: the setup kernel's dynamic shared-memory limit is raised to
 // the maximum once per device (which also loads the kernel); *limit receives it.
@@ -265,7 +270,9 @@ size_t plan_layout(Problem* pb, char* base, size_t* in_offset)
     const bool f32 = pb->f32 != 0;
     size_t o_d32 = f32 ? take(sizeof(float) * terms * n * c) : 0;
     size_t o_mt = take(sizeof(double) * (size_t)(n - 1 - pb->w > 0 ? n - 1 - pb->w : 1) * n * c);
-    size_t o_part = take(sizeof(dd) * (size_t)pb->grid * c);
+    // two per CTA at least: the fused small call keeps its walk totals and its
+    // corrections apart
+    size_t o_part = take(sizeof(dd) * (size_t)pb->grid * (c > 2 ? c : 2));
     size_t o_tick = take(sizeof(unsigned) * 4);
     size_t o_rbk = take(sizeof(Readback));
     size_t o_bnd = take(sizeof(double) * 2 * n);
@@ -418,6 +425,34 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
                                      cudaMemcpyHostToDevice, stream));
         d_a = d_in;
     }
+    dd res[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    int exp_sum = 0, launches = 0;
+    double ms_refine = 0.0;
+    // Small real matrices: the whole call as one cooperative kernel
+    // (small_call.cu), unless the device cannot hold its grid or its count
+    // check fails, in which case the separate kernels below run.
+    bool fused = false;
+    if (opt.small_call >= 0 && comps == 1 && pb.na == n && !pb.f32 && n >= 4 && n <= kSmallCallMaxN &&
+        !opt.replay_listing && pb.units <= (unsigned long long)blocks * threads && pb.units <= kRawCap &&
+        small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin) {
+        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
+        if ((st = launch_small_call(pb, d_a, blocks, threads, stream, &fused)) != SPB_OK) return out->status = st;
+        if (fused) {
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
+            SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
+            SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+            launches = 1;
+            res[0] = dd_add(hrb->res[0], hrb->corr[0]);
+            exp_sum = hrb->exp_sum;
+            if (dd_mode) {
+                out->err_est = hrb->err;
+                out->refined_units = hrb->count;
+                if (hrb->list_n != hrb->count) fused = false;  // run the separate kernels instead
+            }
+        }
+    }
+    if (!fused) {
     // The walk's list bin, written by the setup kernel (which also zeroes the
     // counters and histograms): 0 lists every unit when all fit the list;
     // 0x7f7f7f7f, above every bin, lists none (the row-compacted walk, whose
@@ -427,7 +462,7 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     if ((st = launch_setup(pb, d_a, stream)) != SPB_OK) return out->status = st;
     SPB_CUDA_TRY(cudaGetLastError());
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
-    int launches = 2;
+    launches = 2;
     if (dd_mode && pb.na == n && pb.units > pb.raw_cap / 2) {
         // Size the first pass's unit list from a bound-only pass (about 1.5 %
         // of a dense walk).  The row-compacted walk has few terms per unit, so
@@ -468,9 +503,9 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     }
     if ((st = read_back()) != SPB_OK) return out->status = st;
     const dd res0[2] = {hrb->res[0], hrb->res[1]};
-    dd res[2] = {res0[0], res0[1]};
-    const int exp_sum = hrb->exp_sum;
-    double ms_refine = 0.0;
+    res[0] = res0[0];
+    res[1] = res0[1];
+    exp_sum = hrb->exp_sum;
     if (dd_mode) {
         const unsigned long long count = hrb->count;
         out->err_est = hrb->err;
@@ -518,6 +553,7 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
         ms_refine = mr;
     }
+    }  // separate kernels
     float ms = 0.f, ms_call = 0.f;
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
     SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));

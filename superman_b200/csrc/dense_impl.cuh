@@ -286,8 +286,9 @@ __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const dou
     return acc;
 }
 
-// First unit base of each thread, built cooperatively by its warp; every
-// lane of the warp calls this (it shuffles), whether it owns units or not.
+// First unit base of each thread, built cooperatively by its warp from the
+// NW start vector (x0h, x0l) and the high columns s_mt; every lane of the
+// warp calls this (it shuffles), whether it owns units or not.
 // The lanes' first units u0 lie in one range [ulo, uhi] (balanced_range is
 // monotonic in the thread index), so the Gray bits above P, the highest bit
 // where ulo and uhi differ, are the same for every lane.  Lane r adds the
@@ -299,9 +300,10 @@ __device__ __forceinline__ double unit_sum_real(const double (&xh)[N], const dou
 // every lane adding all of its columns, this saves most of the double-double
 // adds when threads own few units (n <= 26).
 template <int N>
-__device__ __forceinline__ void first_base_real(const Problem& pb, const double* __restrict__ s_mt,
-                                                double* s_lo, int ntop, unsigned long long u0,
-                                                unsigned long long u1, int tid, int bd, double (&xh)[N])
+__device__ __forceinline__ void first_base_real(const double* __restrict__ x0h, const double* __restrict__ x0l,
+                                                const double* __restrict__ s_mt, double* s_lo, int ntop,
+                                                unsigned long long u0, unsigned long long u1, int tid, int bd,
+                                                double (&xh)[N])
 {
     const unsigned full = 0xffffffffu;
     const int lane = tid & 31;
@@ -313,8 +315,8 @@ __device__ __forceinline__ void first_base_real(const Problem& pb, const double*
     const unsigned long long gc = gray_of(ulo);
     dd c0 = {0.0, 0.0}, c1 = {0.0, 0.0};
     if (lane < N) {
-        c0 = dd{pb.x0_hi[lane], pb.x0_lo[lane]};
-        if (N > 32 && lane + 32 < N) c1 = dd{pb.x0_hi[lane + 32], pb.x0_lo[lane + 32]};
+        c0 = dd{x0h[lane], x0l[lane]};
+        if (N > 32 && lane + 32 < N) c1 = dd{x0h[lane + 32], x0l[lane + 32]};
         for (int j = P + 1; j < ntop; ++j)
             if ((gc >> j) & 1ull) {
                 c0 = dd_add_d(c0, s_mt[j * N + lane]);
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(RealCfg<N>::kMaxThreads, 1) walk_real(Problem 
     // ones first (the refinement rebuilds bases in plain index order; the hi
     // words agree unless a row value lies within ~2^-100 of a rounding
     // midpoint, and then only that unit's correction carries one FP64 rounding).
-    first_base_real<N>(pb, s_mt, s_lo, ntop, u0, u1, tid, bd, xh);
+    first_base_real<N>(pb.x0_hi, pb.x0_lo, s_mt, s_lo, ntop, u0, u1, tid, bd, xh);
     if (u0 < u1) {
         unsigned long long u = u0;
         while (true) {

@@ -24,46 +24,11 @@
 
 #include "bound_impl.cuh"
 #include "dense_impl.cuh"
+#include "refine_impl.cuh"
 
 namespace spb {
 namespace dense {
 namespace {
-
-// One group of G terms, bitwise identical to unit_sum_real<N,G>'s group
-// (na == n) or to unit_sum_sparse<NA>'s (na < n: the inactive rows' product
-// first, then the na active rows; see sparse_impl.cuh).  The group's term i
-// of row r is de[r * rs + i].
-__device__ __forceinline__ double group_sum_real_rt(const double* xh, const double* de, int n, int na, int G,
-                                                    int rs)
-{
-    double p0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
-    p0 = add_rn(xh[0], de[0]);
-    if (G >= 2) p1 = add_rn(xh[0], de[1]);
-    if (G == 4) {
-        p2 = add_rn(xh[0], de[2]);
-        p3 = add_rn(xh[0], de[3]);
-    }
-    if (na < n) {
-        double c = xh[na];
-        for (int r = na + 1; r < n; ++r) c = mul_rn(c, xh[r]);
-        p0 = mul_rn(c, p0);
-        p1 = mul_rn(c, p1);
-        p2 = mul_rn(c, p2);
-        p3 = mul_rn(c, p3);
-    }
-    for (int r = 1; r < na; ++r) {
-        const double x = xh[r];
-        p0 = mul_rn(p0, add_rn(x, de[r * rs + 0]));
-        if (G >= 2) p1 = mul_rn(p1, add_rn(x, de[r * rs + 1]));
-        if (G == 4) {
-            p2 = mul_rn(p2, add_rn(x, de[r * rs + 2]));
-            p3 = mul_rn(p3, add_rn(x, de[r * rs + 3]));
-        }
-    }
-    if (G == 4) return sub_rn(sub_rn(p0, p1), sub_rn(p2, p3));
-    if (G == 2) return sub_rn(p0, p1);
-    return p0;
-}
 
 // One group of G (<= 4) complex terms, bitwise identical to unit_sum_complex<N,G>.
 // The group's term i of row r is dr/di[r * rs + i].
@@ -250,92 +215,21 @@ __global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
     if (lane == 0) *pb.list_bin = b;
 }
 
-// Picks the refinement bin: the lowest bin b such that the units below it,
-// left in FP64, have an expected rounding error sqrt(sum t^2 * k/12) * 2^-52
-// (k rounded operations per term) within half the tolerance of the walk's
-// magnitude.  At most 1/8 of the units are refined; past that b moves up and
-// the estimate is reported instead.  Also decides whether the walk's own list
-// holds every unit at or above b (no overflow, b >= its list bin) and resets
-// the list counter.  One warp; lane l owns bins [16l, 16l + 16), and the
-// cumulative sums over bins are lane-local sums joined by warp scans (a fixed
-// order, so the result is deterministic).
+// Picks the refinement bin (pick_threshold, refine_impl.cuh) from the walk's
+// histogram and total.  Also decides whether the walk's own list holds every
+// unit at or above it (no overflow, bin >= its list bin) and resets the list
+// counter.  One warp.
 __global__ void __launch_bounds__(32) dd_threshold(Problem pb)
 {
-    constexpr int kPer = kHistBins / 32;
     const int lane = threadIdx.x;
-    const unsigned full = 0xffffffffu;
     Readback* rb = pb.rb;
-    const double k = pb.comps == 1 ? 2.0 * pb.n : 6.0 * pb.n;
-    const double var_per_s2 = mul_rn(k / 12.0, 0x1p-104);
     const double mag = pb.comps == 1 ? fabs(rb->res[0].hi) : hypot(rb->res[0].hi, rb->res[1].hi);
-    const double half = mul_rn(0.5 * pb.tol, mag);
-    const double budget = mag > 0.0 ? mul_rn(half, half) : 0.0;
-    double v[kPer];
-    unsigned long long cn[kPer];
-    double loc = 0.0;
-    unsigned long long cl = 0;
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        v[i] = mul_rn(pb.hist_s2[lane * kPer + i], var_per_s2);
-        cn[i] = pb.hist_cnt[lane * kPer + i];
-        loc = add_rn(loc, v[i]);
-        cl += cn[i];
-    }
-    // Inclusive prefix of the lanes' sums of v, inclusive suffix of their counts.
-    double incl = loc;
-    unsigned long long sfx = cl;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const double o = __shfl_up_sync(full, incl, d);
-        const unsigned long long p = __shfl_down_sync(full, sfx, d);
-        if (lane >= d) incl = add_rn(incl, o);
-        if (lane + d < 32) sfx += p;
-    }
-    double excl = __shfl_up_sync(full, incl, 1);
-    if (lane == 0) excl = 0.0;
-    unsigned long long after = __shfl_down_sync(full, sfx, 1);  // units in the lanes above
-    if (lane == 31) after = 0;
-    // b0: the first bin whose cumulative sum would exceed the budget.
-    int first = kHistBins;
-    double cum = excl;
-#pragma unroll
-    for (int i = 0; i < kPer; ++i)
-        if (first == kHistBins) {
-            const double next = add_rn(cum, v[i]);
-            if (!(next <= budget)) first = lane * kPer + i;
-            else cum = next;
-        }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) first = min(first, __shfl_xor_sync(full, first, d));
-    // b: the first bin >= b0 whose tail holds at most units/8 units.
-    const unsigned long long cap = pb.units / 8;
-    int bsel = kHistBins;
-    unsigned long long tail = after;  // units in bins >= the current one, walking down
-#pragma unroll
-    for (int i = kPer - 1; i >= 0; --i) {
-        tail += cn[i];
-        const int bin = lane * kPer + i;
-        if (bin >= first && tail <= cap) bsel = bin;
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) bsel = min(bsel, __shfl_xor_sync(full, bsel, d));
-    // The owner of bin bsel (lane 31 for bsel == kHistBins) has the sums below it.
-    const int owner = bsel < kHistBins ? bsel / kPer : 31;
-    double below = excl;
-    unsigned long long from = after;
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        const int bin = lane * kPer + i;
-        if (bin < bsel) below = add_rn(below, v[i]);
-        else from += cn[i];
-    }
-    below = __shfl_sync(full, below, owner);
-    from = __shfl_sync(full, from, owner);
+    const ThresholdPick t = pick_threshold(pb, mag);
     if (lane == 0) {
-        rb->thr = bsel;
-        rb->count = bsel < kHistBins ? from : 0ull;
-        rb->err = mag > 0.0 ? sqrt(below) / mag : INFINITY;
-        rb->from_list = (bsel >= *pb.list_bin && *pb.raw_n <= pb.raw_cap) ? 1 : 0;
+        rb->thr = t.thr;
+        rb->count = t.count;
+        rb->err = t.err;
+        rb->from_list = (t.thr >= *pb.list_bin && *pb.raw_n <= pb.raw_cap) ? 1 : 0;
         rb->list_n = 0;
         // the refinement writes its correction only when it has units
         rb->corr[0] = dd{0.0, 0.0};

@@ -1,0 +1,394 @@
+// One cooperative kernel for a whole dense real permanent of small size
+// (4 <= n <= kSmallCallMaxN), in FP64 mode or with the double-double
+// refinement.
+//
+// At these sizes the Gray walk itself is a few tens of microseconds, and a
+// call made of separate kernels (setup, walk, threshold, listing, refinement)
+// spends about as long again in launches, one-CTA phases and the gaps between
+// kernels.  Here every CTA of a persistent grid (one per SM, launched
+// cooperatively so that all are resident) does the whole call:
+//   0. builds the tables the walk reads in its own shared memory from the
+//      matrix: row scaling by powers of two, the double-double NW start vector
+//      and subset-sum table, the high columns and the per-row bound ranges,
+//      with the operations of setup_kernel, so the values are the same;
+//      CTA 0 also zeroes the call's global accumulators; grid barrier;
+//   1. walks its units exactly as walk_real does (same unit split, same
+//      first-base build, same evaluators), binning each unit by its bound and
+//      recording the bin per unit; CTA totals go to pb.partials; grid barrier;
+//   2. every CTA sums the CTA totals in index order (the grid total, as
+//      grid_reduce forms it) and, with the refinement, picks the threshold
+//      from the histogram (one warp, pick_threshold);
+//   3. with the refinement, each CTA takes every grid-th unit index, keeps the
+//      units at or above the threshold, and its warps re-evaluate them in
+//      double-double against the FP64 value the walk computed (rebuilt base,
+//      same group evaluator), as refine_real does; the last CTA sums the
+//      corrections in index order.
+// The host reads the result back once.  The walk never waits on anything but
+// the two grid barriers of cooperative groups.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "dense_impl.cuh"
+#include "refine_impl.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace spb {
+namespace dense {
+
+constexpr int kSmallCallMaxN = 24;
+constexpr int kSmallCallThreads = 512;
+
+namespace {
+
+__host__ __device__ constexpr size_t even(size_t v) { return (v + 1) & ~(size_t)1; }
+
+// Shared-memory layout, in doubles from the dynamic base; every array
+// starts 16-byte aligned (the evaluators read the table with 16-byte loads).
+struct SmallLayout {
+    size_t a, x0h, x0l, dh, dl, mt, lo, bnd, xw, gw, hist, total;
+    __host__ __device__ SmallLayout(int n, int w, int threads)
+    {
+        const size_t terms = (size_t)1 << w, ntop = n - 1 - w > 0 ? n - 1 - w : 0, nq = terms / 4;
+        const size_t warps = threads / 32;
+        a = 0;
+        x0h = even(a + (size_t)n * n);
+        x0l = even(x0h + n);
+        dh = even(x0l + n);
+        dl = even(dh + terms * n);
+        mt = even(dl + terms * n);
+        lo = even(mt + ntop * n);
+        bnd = even(lo + (size_t)n * threads);
+        xw = even(bnd + 2 * (size_t)n);          // [warps][2n] rebuilt unit bases
+        gw = even(xw + warps * 2 * (size_t)n);    // [warps][nq] FP64 group sums
+        hist = even(gw + warps * nq);             // float[kHistBins] + unsigned[kHistBins]
+        total = hist + (kHistSmemBytes + sizeof(double) - 1) / sizeof(double);
+    }
+    size_t bytes() const { return total * sizeof(double); }
+};
+
+// Sum over the CTA in warp order; valid in thread 0.
+__device__ __forceinline__ dd block_sum_dd(dd v, dd* s_warp)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum_dd(v);
+    if (lane == 0) s_warp[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < nw ? s_warp[lane] : dd{0.0, 0.0};
+        v = warp_sum_dd(v);
+    }
+    __syncthreads();
+    return v;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* __restrict__ a_in)
+{
+    constexpr int G = RealCfg<N>::G;
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_exp[N];
+    __shared__ dd s_warp[32];
+    __shared__ dd s_total;
+    __shared__ int s_thr;
+    __shared__ unsigned long long s_count;
+    __shared__ double s_err;
+    __shared__ unsigned s_nlist;
+    __shared__ unsigned long long s_list[kSmallCallThreads];
+    __shared__ int s_last;
+    const int w = pb.w, terms = 1 << w, nq = terms / G, ntop = N - 1 - w;
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5, nwarps = bd >> 5;
+    const int mode = pb.mode;
+    const SmallLayout L(N, w, bd);
+    double* s_a = smem + L.a;
+    double* s_x0h = smem + L.x0h;
+    double* s_x0l = smem + L.x0l;
+    double* s_dh = smem + L.dh;
+    double* s_dl = smem + L.dl;
+    double* s_mt = smem + L.mt;
+    double* s_lo = smem + L.lo;
+    double* s_bnd = smem + L.bnd;
+    float* s_hist = reinterpret_cast<float*>(smem + L.hist);
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
+
+    // ---- 0. tables (setup_kernel's operations) and the zeroed accumulators
+    for (int i = tid; i < N * N; i += bd) s_a[i] = a_in[i];
+    if (blockIdx.x == 0) {
+        if (tid < 4) pb.ticket[tid] = 0u;
+        if (mode != 0)
+            for (int i = tid; i < kHistBins; i += bd) {
+                pb.hist_s2[i] = 0.0;
+                pb.hist_cnt[i] = 0ull;
+            }
+        if (tid == 0) *pb.list_n = 0ull;
+    }
+    if (mode != 0)
+        for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
+    __syncthreads();
+    for (int r = tid; r < N; r += bd) {
+        double mx = 0.0;
+        for (int j = 0; j < N; ++j) mx = fmax(mx, fabs(s_a[r * N + j]));
+        int e = 0;
+        if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+        s_exp[r] = e;
+    }
+    __syncthreads();
+    for (int i = tid; i < N * N; i += bd) s_a[i] = ldexp(s_a[i], -s_exp[i / N]);
+    __syncthreads();
+    if (blockIdx.x == 0 && tid == 0) {
+        int es = 0;
+        for (int r = 0; r < N; ++r) es += s_exp[r];
+        *pb.exp_sum = es;
+    }
+    for (int r = tid; r < N; r += bd) {
+        dd s = {0.0, 0.0};
+        for (int j = 0; j < N; ++j) s = dd_add_d(s, s_a[r * N + j]);
+        dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
+        dd x = dd_add_d(h, s_a[r * N + (N - 1)]);
+        s_x0h[r] = x.hi;
+        s_x0l[r] = x.lo;
+    }
+    // subset sums level by level: DE[d] = DE[d - 2^k] + a_k, grouped [d/G][r][d%G]
+    auto pos = [&](int d, int r) { return ((d / G) * N + r) * G + (d % G); };
+    for (int r = tid; r < N; r += bd) {
+        s_dh[pos(0, r)] = 0.0;
+        s_dl[pos(0, r)] = 0.0;
+    }
+    for (int k = 0; k < w; ++k) {
+        __syncthreads();
+        const int half = 1 << k;
+        for (int idx = tid; idx < half * N; idx += bd) {
+            const int d = half + idx / N, r = idx % N;
+            const int from = pos(d - half, r);
+            const dd s = dd_add_d(dd{s_dh[from], s_dl[from]}, s_a[r * N + k]);
+            s_dh[pos(d, r)] = s.hi;
+            s_dl[pos(d, r)] = s.lo;
+        }
+    }
+    if (mode != 0)
+        for (int r = tid; r < N; r += bd) {
+            double lo = 0.0, hi = 0.0;
+            for (int j = 0; j < w; ++j) {
+                const double v = s_a[r * N + j];
+                if (v < 0.0) lo += v; else hi += v;
+            }
+            s_bnd[r] = lo;
+            s_bnd[N + r] = hi;
+        }
+    for (int idx = tid; idx < ntop * N; idx += bd) {
+        const int j = idx / N, r = idx % N;
+        s_mt[idx] = s_a[r * N + (w + j)];
+    }
+    __syncthreads();
+    grid.sync();  // the zeroed accumulators are visible before anyone adds to them
+
+    // ---- 1. the walk (walk_real's body on the shared tables)
+    const unsigned long long T = (unsigned long long)gridDim.x * bd;
+    const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
+    unsigned long long u0, u1;
+    balanced_range(pb.units, T, t, &u0, &u1);
+    dd tot = {0.0, 0.0};
+    HistCache hc;
+    double xh[N];
+    first_base_real<N>(s_x0h, s_x0l, s_mt, s_lo, ntop, u0, u1, tid, bd, xh);
+    if (u0 < u1) {
+        unsigned long long u = u0;
+        while (true) {
+            if (mode == 0) {
+                const double us = unit_sum_real<N, G>(xh, s_dh, nq);
+                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+            } else {
+                double ub = 1.0;
+#pragma unroll
+                for (int r = 0; r < N; ++r)
+                    ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
+                const int b = hist_bin(ub);
+                pb.raw_b[u] = (unsigned short)b;
+                double sq;
+                const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
+                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+                hc.add(b, sq, s_hist, s_cnt);
+            }
+            if (++u >= u1) break;
+            const int j = __ffsll((long long)u) - 1;
+            const bool add = (gray_of(u) >> j) & 1ull;
+            const double* col = s_mt + j * N;
+#pragma unroll
+            for (int r = 0; r < N; ++r) {
+                const double m = add ? col[r] : -col[r];
+                const dd s = two_sum(xh[r], m);
+                const dd z = fast_two_sum(s.hi, add_rn(s.lo, s_lo[r * bd + tid]));
+                xh[r] = z.hi;
+                s_lo[r * bd + tid] = z.lo;
+            }
+        }
+    }
+    if (mode != 0) {
+        hc.flush(s_hist, s_cnt);
+        __syncthreads();
+        flush_hist(s_hist, s_cnt, pb);
+    }
+    // CTA total, reduced as grid_reduce does
+    const dd cta = block_sum_dd(tot, s_warp);
+    if (tid == 0) pb.partials[blockIdx.x] = cta;
+    grid.sync();
+
+    // ---- 2. grid total (index order, every CTA alike) and the threshold
+    if (wid == 0) {
+        dd v = {0.0, 0.0};
+        for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + b));
+        v = warp_sum_dd(v);
+        if (lane == 0) s_total = v;
+        if (mode != 0) {
+            const double mag = fabs(v.hi);
+            const ThresholdPick pk = pick_threshold(pb, mag);
+            if (lane == 0) {
+                s_thr = pk.thr;
+                s_count = pk.count;
+                s_err = pk.err;
+            }
+        }
+    }
+    if (tid == 0) s_nlist = 0u;
+    __syncthreads();
+    if (blockIdx.x == 0 && tid == 0) {
+        pb.rb->res[0] = s_total;
+        pb.rb->corr[0] = dd{0.0, 0.0};
+        if (mode != 0) {
+            pb.rb->thr = s_thr;
+            pb.rb->count = s_count;
+            pb.rb->err = s_err;
+            pb.rb->from_list = 1;
+        }
+    }
+    if (mode == 0 || s_thr >= kHistBins) return;  // nothing to refine (uniform over the grid)
+
+    // ---- 3. refinement of the units at or above the threshold
+    const int thr = s_thr;
+    for (unsigned long long u = (unsigned long long)blockIdx.x * bd + tid; u < pb.units; u += T)
+        if ((int)pb.raw_b[u] >= thr) s_list[atomicAdd(&s_nlist, 1u)] = u;
+    __syncthreads();
+    const unsigned nl = s_nlist;
+    double* xw = smem + L.xw + (size_t)wid * 2 * N;
+    double* gw = smem + L.gw + (size_t)wid * nq;
+    dd corr = {0.0, 0.0};
+    for (unsigned k = wid; k < nl; k += nwarps) {
+        const unsigned long long u = s_list[k];
+        const unsigned long long g = gray_of(u);
+        // unit base rebuilt from scratch in double-double (x0 plus the
+        // selected high columns in index order), as refine_real does
+        for (int r = lane; r < N; r += 32) {
+            dd x = {s_x0h[r], s_x0l[r]};
+            for (int j = 0; j < ntop; ++j)
+                if ((g >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
+            xw[r] = x.hi;
+            xw[N + r] = x.lo;
+        }
+        __syncwarp();
+        for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * (N * G), N, N, G, G);
+        dd acc = {0.0, 0.0};
+        for (int d = lane; d < terms; d += 32) {
+            dd p = dd_add(dd{xw[0], xw[N]}, dd{s_dh[pos(d, 0)], s_dl[pos(d, 0)]});
+            for (int r = 1; r < N; ++r)
+                p = dd_mul(p, dd_add(dd{xw[r], xw[N + r]}, dd{s_dh[pos(d, r)], s_dl[pos(d, r)]}));
+            acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
+        }
+        acc = warp_sum_dd(acc);
+        __syncwarp();
+        if (lane == 0) {
+            double f = 0.0;
+            for (int q = 0; q < nq; ++q) f = (__popc(q) & 1) ? sub_rn(f, gw[q]) : add_rn(f, gw[q]);
+            dd c = dd_add_d(acc, -f);
+            if (u & 1ull) c = dd_neg(c);
+            corr = dd_add(corr, c);
+        }
+        __syncwarp();
+    }
+    const dd cc = block_sum_dd(corr, s_warp);
+    if (tid == 0) {
+        pb.partials[gridDim.x + blockIdx.x] = cc;
+        atomicAdd(pb.list_n, (unsigned long long)nl);
+        __threadfence();
+        const unsigned prev = atomicAdd(pb.ticket, 1u);
+        s_last = prev == gridDim.x - 1 ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last && wid == 0) {
+        __threadfence();
+        dd v = {0.0, 0.0};
+        for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + gridDim.x + b));
+        v = warp_sum_dd(v);
+        if (lane == 0) {
+            pb.rb->corr[0] = v;
+            *pb.ticket = 0u;
+        }
+    }
+}
+
+using SmallKernel = void (*)(Problem, const double*);
+
+SmallKernel small_kernel(int n)
+{
+    switch (n) {
+#define SPB_SCASE(N) \
+    case N: return small_call_real<N>;
+        SPB_SCASE(4) SPB_SCASE(5) SPB_SCASE(6) SPB_SCASE(7) SPB_SCASE(8) SPB_SCASE(9) SPB_SCASE(10)
+        SPB_SCASE(11) SPB_SCASE(12) SPB_SCASE(13) SPB_SCASE(14) SPB_SCASE(15) SPB_SCASE(16)
+        SPB_SCASE(17) SPB_SCASE(18) SPB_SCASE(19) SPB_SCASE(20) SPB_SCASE(21) SPB_SCASE(22)
+        SPB_SCASE(23) SPB_SCASE(24)
+#undef SPB_SCASE
+    default: return nullptr;
+    }
+}
+
+}  // namespace
+
+size_t small_call_smem_bytes(int n, int w, int threads) { return SmallLayout(n, w, threads).bytes(); }
+
+// Launches the fused call if this device can keep `blocks` CTAs of it
+// resident at once; *launched tells whether it did.
+int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, cudaStream_t s, bool* launched)
+{
+    *launched = false;
+    SmallKernel kern = small_kernel(pb.n);
+    if (!kern || threads != kSmallCallThreads) return SPB_OK;
+    const size_t smem = small_call_smem_bytes(pb.n, pb.w, threads);
+    static std::mutex mu;
+    static int fits[64][kSmallCallMaxN + 1];  // 0 unknown, 1 fits, -1 does not
+    int dev = 0;
+    SPB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return SPB_OK;
+    int sms = 0;
+    SPB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (fits[dev][pb.n] == 0) {
+            int optin = 0, coop = 0, per_sm = 0;
+            cudaFuncAttributes fa{};
+            SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            SPB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+            SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+            fits[dev][pb.n] = -1;
+            if (coop && smem + fa.sharedSizeBytes <= (size_t)optin) {
+                SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  optin - (int)fa.sharedSizeBytes));
+                SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+                if (per_sm >= 1) fits[dev][pb.n] = 1;
+            }
+        }
+        if (fits[dev][pb.n] < 0) return SPB_OK;
+    }
+    if (blocks > sms) return SPB_OK;  // one CTA per SM must hold the whole grid
+    Problem p = pb;
+    const double* a = d_a;
+    void* args[] = {&p, &a};
+    SPB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(blocks), dim3(threads), args, smem, s));
+    *launched = true;
+    return SPB_OK;
+}
+
+}  // namespace dense
+}  // namespace spb

@@ -1,0 +1,78 @@
+"""The fused small-matrix call (one cooperative kernel for real 4 <= n <= 24:
+tables, walk, threshold and double-double refinement) against the same call
+made of separate kernels, and against the exact value."""
+import numpy as np
+import pytest
+
+from superman_b200 import workloads as W
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [4, 5, 9, 13, 17, 20, 22, 24])
+def test_fused_equals_separate_fp64(spb, n):
+    """FP64 mode: the same walk, unit split and reduction order, so the same
+    bits."""
+    a = W.dense_uniform(n, 700 + n)
+    f = spb.perm_dense(a, precision="fp64")
+    s = spb.perm_dense(a, precision="fp64", small_call=-1)
+    assert f.launches == 1 and s.launches >= 2
+    assert (f.permanent, f.permanent_lo) == (s.permanent, s.permanent_lo)
+
+
+@pytest.mark.parametrize("n", [6, 12, 18, 21, 24])
+def test_fused_dd_matches_separate_and_exact(spb, oracle, n):
+    a = W.dense_uniform(n, 710 + n)
+    f = spb.perm_dense(a, precision="dd")
+    s = spb.perm_dense(a, precision="dd", small_call=-1)
+    assert f.launches == 1
+    assert f.refined_units == s.refined_units
+    assert abs(f.permanent - s.permanent) <= 1e-15 * abs(s.permanent)
+    assert oracle.rel_err(f.permanent + f.permanent_lo, oracle.exact_perm(a)) <= 1e-13
+
+
+def test_fused_dd_golden_n24(spb, oracle):
+    a, exact, _ = load_golden("dense_u01_n24_s3")
+    f = spb.perm_dense(a, precision="dd")
+    assert f.launches == 1 and f.refined_units > 0
+    assert oracle.rel_err(f.permanent, exact) <= 1e-13
+
+
+def test_fused_dd_forced_refinement_signed(spb, oracle):
+    """Signed entries and a tight tolerance: many units refined inside the
+    fused call, still exact to the bar."""
+    rng = np.random.default_rng(31)
+    a = rng.standard_normal((20, 20))
+    f = spb.perm_dense(a, precision="dd", rel_tol=1e-16)
+    s = spb.perm_dense(a, precision="dd", rel_tol=1e-16, small_call=-1)
+    assert f.launches == 1 and f.refined_units == s.refined_units > 0
+    exact = oracle.exact_perm(a)
+    assert oracle.rel_err(f.permanent, exact) <= 1e-12
+    assert abs(f.permanent - s.permanent) <= 1e-14 * abs(exact)
+
+
+def test_fused_device_input_and_edge_values(spb):
+    """Device-resident input, a zero row (permanent 0) and rows scaled far
+    apart go through the fused call like the separate kernels."""
+    import ctypes
+    import torch
+    from superman_b200 import _lib
+    a = W.dense_uniform(16, 3)
+    d = torch.from_numpy(a).cuda()
+    out = _lib.spb_result()
+    opt = _lib.default_options(precision=_lib.SPB_PREC_DD)
+    _lib.check(_lib.lib().spb_perm_dense_f64_dev(ctypes.c_void_p(d.data_ptr()), 16, ctypes.byref(opt),
+                                                 ctypes.byref(out)))
+    assert out.launches == 1
+    want = spb.perm_dense(a, precision="dd", small_call=-1).permanent
+    assert abs(out.value - want) <= 1e-15 * abs(want)
+    z = W.dense_uniform(14, 4)
+    z[5] = 0.0
+    assert spb.perm_dense(z, sparse_walk=1).permanent == 0.0
+    sc = np.full((12, 12), 0.75)
+    sc[:6] *= 2.0 ** 900
+    sc[6:] *= 2.0 ** -900
+    r = spb.perm_dense(sc, precision="dd")
+    import math
+    assert abs(r.permanent - math.factorial(12) * 0.75 ** 12) <= 1e-13 * r.permanent
