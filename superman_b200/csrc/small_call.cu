@@ -18,13 +18,13 @@
 //   2. every CTA sums the CTA totals in index order (the grid total, as
 //      grid_reduce forms it) and, with the refinement, picks the threshold
 //      from the histogram (one warp, pick_threshold);
-//   3. with the refinement, each CTA takes every grid-th unit index, keeps the
-//      units at or above the threshold, and its warps re-evaluate them in
-//      double-double against the FP64 value the walk computed (rebuilt base,
-//      same group evaluator), as refine_real does; the last CTA sums the
-//      corrections in index order.
-// The host reads the result back once.  The walk never waits on anything but
-// the two grid barriers of cooperative groups.
+//   3. with the refinement, each CTA lists the units of its slice at or above
+//      the threshold; grid barrier; the listed units are dealt out one per CTA
+//      and re-evaluated by the whole CTA in double-double against the FP64
+//      value the walk computed (rebuilt base, same group evaluator), as
+//      refine_real does; the last CTA sums the corrections in index order.
+// The host reads the result back once.  Nothing waits on anything but the
+// grid barriers of cooperative groups.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -96,11 +96,9 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __shared__ int s_thr;
     __shared__ unsigned long long s_count;
     __shared__ double s_err;
-    __shared__ unsigned s_nlist;
-    __shared__ unsigned long long s_list[kSmallCallThreads];
     __shared__ int s_last;
     const int w = pb.w, terms = 1 << w, nq = terms / G, ntop = N - 1 - w;
-    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5, nwarps = bd >> 5;
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5;
     const int mode = pb.mode;
     const SmallLayout L(N, w, bd);
     double* s_a = smem + L.a;
@@ -252,7 +250,6 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
             }
         }
     }
-    if (tid == 0) s_nlist = 0u;
     __syncthreads();
     if (blockIdx.x == 0 && tid == 0) {
         pb.rb->res[0] = s_total;
@@ -266,51 +263,63 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     }
     if (mode == 0 || s_thr >= kHistBins) return;  // nothing to refine (uniform over the grid)
 
-    // ---- 3. refinement of the units at or above the threshold
+    // ---- 3. refinement of the units at or above the threshold.  Each CTA
+    // lists the units of its slice; after a grid barrier the listed units
+    // are dealt out one per CTA in list order, so a cluster of dominant units
+    // (they gather near the empty and the full subsets) spreads over the grid,
+    // and each is refined by a whole CTA.
     const int thr = s_thr;
     for (unsigned long long u = (unsigned long long)blockIdx.x * bd + tid; u < pb.units; u += T)
-        if ((int)pb.raw_b[u] >= thr) s_list[atomicAdd(&s_nlist, 1u)] = u;
-    __syncthreads();
-    const unsigned nl = s_nlist;
-    double* xw = smem + L.xw + (size_t)wid * 2 * N;
-    double* gw = smem + L.gw + (size_t)wid * nq;
+        if ((int)pb.raw_b[u] >= thr) {
+            const unsigned long long k = atomicAdd(pb.list_n, 1ull);
+            if (k < pb.list_cap) pb.list_u[k] = u;
+        }
+    grid.sync();
+    const unsigned long long listed = __ldcg(pb.list_n);
+    const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
+    double* xw = smem + L.xw;  // [2N]: the unit base, hi then lo
+    double* gw = smem + L.gw;  // [nq]: the walk's FP64 group sums
+    // threads per term: a power of two up to a warp; each takes a run of rows
+    const int per = bd >= 32 * terms ? 32 : (bd >= terms ? bd / terms : 1);
+    const int sub = tid % per, r0 = sub * N / per, r1 = (sub + 1) * N / per;
     dd corr = {0.0, 0.0};
-    for (unsigned k = wid; k < nl; k += nwarps) {
-        const unsigned long long u = s_list[k];
+    for (unsigned long long k = blockIdx.x; k < nl; k += gridDim.x) {
+        const unsigned long long u = __ldcg(pb.list_u + k);
         const unsigned long long g = gray_of(u);
         // unit base rebuilt from scratch in double-double (x0 plus the
         // selected high columns in index order), as refine_real does
-        for (int r = lane; r < N; r += 32) {
+        for (int r = tid; r < N; r += bd) {
             dd x = {s_x0h[r], s_x0l[r]};
             for (int j = 0; j < ntop; ++j)
                 if ((g >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
             xw[r] = x.hi;
             xw[N + r] = x.lo;
         }
-        __syncwarp();
-        for (int q = lane; q < nq; q += 32) gw[q] = group_sum_real_rt(xw, s_dh + q * (N * G), N, N, G, G);
+        __syncthreads();
+        // the unit's FP64 value exactly as the walk computed it, group by group
+        for (int q = tid; q < nq; q += bd) gw[q] = group_sum_real_rt(xw, s_dh + q * (N * G), N, N, G, G);
+        // its double-double value: each term's product over the rows of
+        // `per` threads, joined by shuffles
         dd acc = {0.0, 0.0};
-        for (int d = lane; d < terms; d += 32) {
-            dd p = dd_add(dd{xw[0], xw[N]}, dd{s_dh[pos(d, 0)], s_dl[pos(d, 0)]});
-            for (int r = 1; r < N; ++r)
+        for (int d = tid / per; d < terms; d += bd / per) {
+            dd p = {1.0, 0.0};
+            for (int r = r0; r < r1; ++r)
                 p = dd_mul(p, dd_add(dd{xw[r], xw[N + r]}, dd{s_dh[pos(d, r)], s_dl[pos(d, r)]}));
-            acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
+            for (int off = 1; off < per; off <<= 1) p = dd_mul(p, shfl_xor_dd(p, off));
+            if (sub == 0) acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
         }
-        acc = warp_sum_dd(acc);
-        __syncwarp();
-        if (lane == 0) {
+        acc = block_sum_dd(acc, s_warp);  // also orders gw's writes before thread 0 reads them
+        if (tid == 0) {
             double f = 0.0;
             for (int q = 0; q < nq; ++q) f = (__popc(q) & 1) ? sub_rn(f, gw[q]) : add_rn(f, gw[q]);
             dd c = dd_add_d(acc, -f);
             if (u & 1ull) c = dd_neg(c);
             corr = dd_add(corr, c);
         }
-        __syncwarp();
+        __syncthreads();  // xw and gw are rewritten by the next unit
     }
-    const dd cc = block_sum_dd(corr, s_warp);
     if (tid == 0) {
-        pb.partials[gridDim.x + blockIdx.x] = cc;
-        atomicAdd(pb.list_n, (unsigned long long)nl);
+        pb.partials[gridDim.x + blockIdx.x] = corr;
         __threadfence();
         const unsigned prev = atomicAdd(pb.ticket, 1u);
         s_last = prev == gridDim.x - 1 ? 1 : 0;
