@@ -192,6 +192,7 @@ int ensure_pinned(DeviceContext* ctx, size_t bytes)
     if (bytes <= ctx->pinned_bytes) return SPB_OK;
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     ctx->pinned = nullptr;
+    ctx->pinned_dev = nullptr;
     ctx->pinned_bytes = 0;
     size_t want = align_up(bytes < (1u << 16) ? (1u << 16) : bytes, 1u << 16);
     if (cudaMallocHost(&ctx->pinned, want) != cudaSuccess) {
@@ -200,6 +201,12 @@ int ensure_pinned(DeviceContext* ctx, size_t bytes)
         return SPB_ERR_OOM;
     }
     ctx->pinned_bytes = want;
+    // page-locked memory is mapped into the device's address space under
+    // unified addressing; kernels may then write results straight into it
+    if (cudaHostGetDevicePointer(&ctx->pinned_dev, ctx->pinned, 0) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->pinned_dev = nullptr;
+    }
     return SPB_OK;
 }
 

@@ -25,6 +25,7 @@ struct DeviceContext {
     size_t scratch_bytes = 0;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    void* pinned_dev = nullptr;  // the device's address of `pinned` (null if it has none)
     std::mutex mu;  // serialises calls that use this context
 };
 

@@ -186,7 +186,8 @@ size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * 
 // The fused small-matrix call (small_call.cu).
 constexpr int kSmallCallMaxN = 24;
 size_t small_call_smem_bytes(int n, int w, int threads);
-int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, cudaStream_t s, bool* launched);
+int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, Readback* rb_host, int dev,
+                      int sms, cudaStream_t s, bool* launched);
 
 // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
 // subset-sum table: the setup kernel's dynamic shared-memory limit is raised to
@@ -388,6 +389,21 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         spb_set_error("dense n=%d: %zu B shared memory exceeds the %zu B limit", n, smem, ctx->smem_optin);
         return out->status = SPB_ERR_INVALID;
     }
+    // The fused small call (below) walks with fewer threads per CTA on every
+    // SM when the units would leave SMs idle at full CTAs (n = 19 .. 24:
+    // 2^15 or 2^16 units fill 64 or 128 CTAs of 512 threads; 147 CTAs of 448
+    // threads give each SM an eighth less to walk).
+    const bool small_candidate = opt.small_call >= 0 && comps == 1 && pb.na == n && !pb.f32 && n >= 4 &&
+                                 n <= kSmallCallMaxN && !opt.replay_listing;
+    if (small_candidate && opt.threads_per_block <= 0 && opt.blocks <= 0 &&
+        pb.units >= 256ull * (unsigned long long)ctx->sm_count) {
+        const unsigned long long per_sm = (pb.units + ctx->sm_count - 1) / ctx->sm_count;
+        const int t = (int)((per_sm + 31) / 32 * 32);
+        if (t <= threads) {
+            threads = t;
+            smem = smem_for(threads);
+        }
+    }
     int blocks = opt.blocks > 0 ? opt.blocks : ctx->sm_count;
     // never launch more threads than units
     unsigned long long max_blocks = (pb.units + threads - 1) / threads;
@@ -432,15 +448,20 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     // (small_call.cu), unless the device cannot hold its grid or its count
     // check fails, in which case the separate kernels below run.
     bool fused = false;
-    if (opt.small_call >= 0 && comps == 1 && pb.na == n && !pb.f32 && n >= 4 && n <= kSmallCallMaxN &&
-        !opt.replay_listing && pb.units <= (unsigned long long)blocks * threads && pb.units <= kRawCap &&
+    if (small_candidate && pb.units <= (unsigned long long)blocks * threads && pb.units <= kRawCap &&
         small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin) {
+        // The kernel writes the finished readback straight into the pinned
+        // buffer when the device can address it (no copy after the kernel).
+        Readback* mapped = static_cast<Readback*>(ctx->pinned_dev);
         SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
-        if ((st = launch_small_call(pb, d_a, blocks, threads, stream, &fused)) != SPB_OK) return out->status = st;
+        if ((st = launch_small_call(pb, d_a, blocks, threads, mapped, ctx->device, ctx->sm_count, stream,
+                                    &fused)) != SPB_OK)
+            return out->status = st;
         if (fused) {
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
-            SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
+            if (!mapped)
+                SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
             SPB_CUDA_TRY(cudaStreamSynchronize(stream));
             launches = 1;
             res[0] = dd_add(hrb->res[0], hrb->corr[0]);

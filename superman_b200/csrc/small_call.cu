@@ -23,8 +23,10 @@
 //      and re-evaluated by the whole CTA in double-double against the FP64
 //      value the walk computed (rebuilt base, same group evaluator), as
 //      refine_real does; the last CTA sums the corrections in index order.
-// The host reads the result back once.  Nothing waits on anything but the
-// grid barriers of cooperative groups.
+// The last CTA to finish copies the readback into page-locked host memory
+// mapped into the device's address space, so the host copies nothing after
+// the kernel.  Nothing waits on anything but the grid barriers of
+// cooperative groups.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -84,8 +86,23 @@ __device__ __forceinline__ dd block_sum_dd(dd v, dd* s_warp)
     return v;
 }
 
+// Copies the finished readback to the host's page-locked copy (mapped into
+// the device's address space), reading it through L2: its fields were
+// written by other CTAs.  The host then needs no copy after the kernel.
+__device__ __forceinline__ void publish(const Problem& pb, Readback* host)
+{
+    if (!host) return;
+    __threadfence();
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(pb.rb);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(host);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(Readback) / sizeof(unsigned long long)); ++i) dst[i] = __ldcg(src + i);
+}
+static_assert(sizeof(Readback) % sizeof(unsigned long long) == 0, "readback copied in 8-byte words");
+
 template <int N>
-__global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* __restrict__ a_in)
+__global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* __restrict__ a_in,
+                                                                         Readback* rb_host)
 {
     constexpr int G = RealCfg<N>::G;
     cg::grid_group grid = cg::this_grid();
@@ -225,7 +242,34 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         }
     }
     if (mode != 0) {
-        hc.flush(s_hist, s_cnt);
+        // Each thread walked at most one unit, and neighbouring units share
+        // bins, so the lanes of a warp with the same bin are summed by
+        // shuffles first and one shared atomic per bin and warp is issued.
+        const unsigned full = 0xffffffffu;
+        const int b = hc.cnt ? hc.bin : -1;
+        float v = 0.0f;
+        if (hc.cnt) {
+            const double h = hist_half_unscale(hc.bin);
+            v = __double2float_rn((hc.s2 * h) * h);
+        }
+        unsigned pending = __ballot_sync(full, b >= 0);
+        while (pending) {
+            const int leader = __ffs(pending) - 1;
+            const int lb = __shfl_sync(full, b, leader);
+            const bool mine = b == lb;
+            float x = mine ? v : 0.0f;
+            unsigned c = mine ? hc.cnt : 0u;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                x += __shfl_xor_sync(full, x, off);
+                c += __shfl_xor_sync(full, c, off);
+            }
+            if (lane == leader) {
+                atomicAdd(&s_hist[lb], x);
+                atomicAdd(&s_cnt[lb], c);
+            }
+            pending &= ~__ballot_sync(full, mine);
+        }
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
     }
@@ -260,6 +304,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
             pb.rb->err = s_err;
             pb.rb->from_list = 1;
         }
+        if (mode == 0 || s_thr >= kHistBins) publish(pb, rb_host);
     }
     if (mode == 0 || s_thr >= kHistBins) return;  // nothing to refine (uniform over the grid)
 
@@ -279,8 +324,11 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
     double* xw = smem + L.xw;  // [2N]: the unit base, hi then lo
     double* gw = smem + L.gw;  // [nq]: the walk's FP64 group sums
-    // threads per term: a power of two up to a warp; each takes a run of rows
-    const int per = bd >= 32 * terms ? 32 : (bd >= terms ? bd / terms : 1);
+    // threads per term: a power of two up to a warp (so a term's threads are
+    // lanes of one warp and every warp's terms are all in range or all out),
+    // as many as the CTA holds for all terms at once; each takes a run of rows
+    int per = 1;
+    while (per < 32 && 2 * per * terms <= bd) per *= 2;
     const int sub = tid % per, r0 = sub * N / per, r1 = (sub + 1) * N / per;
     dd corr = {0.0, 0.0};
     for (unsigned long long k = blockIdx.x; k < nl; k += gridDim.x) {
@@ -333,11 +381,12 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         if (lane == 0) {
             pb.rb->corr[0] = v;
             *pb.ticket = 0u;
+            publish(pb, rb_host);
         }
     }
 }
 
-using SmallKernel = void (*)(Problem, const double*);
+using SmallKernel = void (*)(Problem, const double*, Readback*);
 
 SmallKernel small_kernel(int n)
 {
@@ -357,43 +406,51 @@ SmallKernel small_kernel(int n)
 
 size_t small_call_smem_bytes(int n, int w, int threads) { return SmallLayout(n, w, threads).bytes(); }
 
-// Launches the fused call if this device can keep `blocks` CTAs of it
-// resident at once; *launched tells whether it did.
-int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, cudaStream_t s, bool* launched)
+// Launches the fused call on device `dev` (the current one, with `sms`
+// SMs) if it can keep `blocks` CTAs of `threads` threads resident at once;
+// *launched tells whether it did.  rb_host (may be null): the device's
+// address of a page-locked copy of the readback, which the kernel fills last.
+int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, Readback* rb_host, int dev,
+                      int sms, cudaStream_t s, bool* launched)
 {
     *launched = false;
     SmallKernel kern = small_kernel(pb.n);
-    if (!kern || threads != kSmallCallThreads) return SPB_OK;
+    if (!kern || threads > kSmallCallThreads || threads < 32 || threads % 32 != 0) return SPB_OK;
+    if (dev < 0 || dev >= 64 || blocks > sms) return SPB_OK;  // one CTA per SM must hold the whole grid
     const size_t smem = small_call_smem_bytes(pb.n, pb.w, threads);
     static std::mutex mu;
-    static int fits[64][kSmallCallMaxN + 1];  // 0 unknown, 1 fits, -1 does not
-    int dev = 0;
-    SPB_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return SPB_OK;
-    int sms = 0;
-    SPB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    static int fits[64][kSmallCallMaxN + 1];  // 0 unknown, 1 kernel configured, -1 cannot run
+    static signed char resident[64][kSmallCallMaxN + 1][kSmallCallThreads / 32 + 1];  // 0 unknown, 1, -1
     {
         std::lock_guard<std::mutex> lk(mu);
         if (fits[dev][pb.n] == 0) {
-            int optin = 0, coop = 0, per_sm = 0;
+            int optin = 0, coop = 0;
             cudaFuncAttributes fa{};
             SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
             SPB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
             SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
             fits[dev][pb.n] = -1;
-            if (coop && smem + fa.sharedSizeBytes <= (size_t)optin) {
+            if (coop) {
                 SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   optin - (int)fa.sharedSizeBytes));
-                SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-                if (per_sm >= 1) fits[dev][pb.n] = 1;
+                fits[dev][pb.n] = 1;
             }
         }
         if (fits[dev][pb.n] < 0) return SPB_OK;
+        // one CTA of this shape must fit an SM (shared memory, registers);
+        // asked once per device, size and shape
+        signed char& res = resident[dev][pb.n][threads / 32];
+        if (res == 0) {
+            int per_sm = 0;
+            SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+            res = per_sm >= 1 ? 1 : -1;
+        }
+        if (res < 0) return SPB_OK;
     }
-    if (blocks > sms) return SPB_OK;  // one CTA per SM must hold the whole grid
     Problem p = pb;
     const double* a = d_a;
-    void* args[] = {&p, &a};
+    Readback* h = rb_host;
+    void* args[] = {&p, &a, &h};
     SPB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(blocks), dim3(threads), args, smem, s));
     *launched = true;
     return SPB_OK;

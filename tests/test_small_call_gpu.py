@@ -12,13 +12,39 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("n", [4, 5, 9, 13, 17, 20, 22, 24])
 def test_fused_equals_separate_fp64(spb, n):
-    """FP64 mode: the same walk, unit split and reduction order, so the same
-    bits."""
+    """FP64 mode at one launch shape: the same walk, unit split and reduction
+    order, so the same bits.  At the default shapes (the fused call spreads
+    n >= 19 over every SM with smaller CTAs) the unit split differs, so only
+    the value is compared."""
     a = W.dense_uniform(n, 700 + n)
-    f = spb.perm_dense(a, precision="fp64")
-    s = spb.perm_dense(a, precision="fp64", small_call=-1)
+    f = spb.perm_dense(a, precision="fp64", threads_per_block=448, blocks=148)
+    s = spb.perm_dense(a, precision="fp64", threads_per_block=448, blocks=148, small_call=-1)
     assert f.launches == 1 and s.launches >= 2
     assert (f.permanent, f.permanent_lo) == (s.permanent, s.permanent_lo)
+    fd = spb.perm_dense(a, precision="fp64")
+    sd = spb.perm_dense(a, precision="fp64", small_call=-1)
+    assert fd.launches == 1
+    assert abs(fd.permanent - sd.permanent) <= 1e-13 * abs(sd.permanent)
+
+
+@pytest.mark.parametrize("n,threads", [(12, 96), (20, 160), (20, 384), (22, 448), (24, 448), (24, 384)])
+def test_fused_launch_shapes(spb, oracle, n, threads):
+    """CTAs of fewer threads: the fused call runs whenever every unit has a
+    thread of the one-CTA-per-SM grid, and is exact to the bar either way."""
+    import torch
+    a = W.dense_uniform(n, 720 + n)
+    r = spb.perm_dense(a, precision="dd", threads_per_block=threads)
+    w = 8  # the library's default unit width: a 64 KB table, >= 2^16 units when n allows
+    while w > 2 and (1 << w) * n * 8 > 64 * 1024:
+        w -= 1
+    while w > 2 and n - 1 - w < 16 and w > n - 17:
+        w -= 1
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    if 2 ** (n - 1 - w) <= sms * threads:
+        assert r.launches == 1
+    else:
+        assert r.launches >= 2
+    assert oracle.rel_err(r.permanent + r.permanent_lo, oracle.exact_perm(a)) <= 1e-13
 
 
 @pytest.mark.parametrize("n", [6, 12, 18, 21, 24])
