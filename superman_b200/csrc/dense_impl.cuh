@@ -184,6 +184,23 @@ __device__ __forceinline__ dd ldcg_dd(const dd* p)
     return {__ldcg(&p->hi), __ldcg(&p->lo)};
 }
 
+// p[lane] + p[lane + 32] + ... over the entries below count, added in that
+// order; the loads (through L2) are issued eight at a time ahead of the adds,
+// so a lane waits for one round trip per eight entries, not one per entry.
+__device__ __forceinline__ dd lane_sum_dd(const dd* p, int count, int lane)
+{
+    dd v = {0.0, 0.0};
+    for (int b0 = lane; b0 < count; b0 += 32 * 8) {
+        dd x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = b0 + 32 * k < count ? ldcg_dd(p + b0 + 32 * k) : dd{0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (b0 + 32 * k < count) v = dd_add(v, x[k]);
+    }
+    return v;
+}
+
 // Warp -> block -> grid double-double reduction of C components.  The last
 // CTA to finish (ticket election) sums the per-CTA partials in index order,
 // so the result does not depend on CTA completion order.
@@ -218,8 +235,7 @@ __device__ __forceinline__ void grid_reduce(dd (&tot)[C], const Problem& pb)
         __threadfence();
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            dd v = {0.0, 0.0};
-            for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + c * pb.grid + b));
+            dd v = lane_sum_dd(pb.partials + c * pb.grid, (int)gridDim.x, lane);
             v = warp_sum_dd(v);
             if (lane == 0) pb.result[c] = v;
         }

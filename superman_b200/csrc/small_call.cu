@@ -12,13 +12,17 @@
 //      and subset-sum table, the high columns and the per-row bound ranges,
 //      with the operations of setup_kernel, so the values are the same;
 //      CTA 0 also zeroes the call's global accumulators; grid barrier;
-//   1. walks its units exactly as walk_real does (same unit split, same
-//      first-base build, same evaluators), binning each unit by its bound and
-//      recording the bin per unit; CTA totals go to pb.partials; grid barrier;
+//   1. evaluates one unit per thread (thread t owns unit t, the split
+//      walk_real makes when there are no more units than threads) with
+//      walk_real's evaluators, on unit bases its warp builds row-parallel
+//      (double-double, so their hi words are walk_real's but for values
+//      within ~2^-104 of a rounding midpoint), binning each unit by its
+//      bound and recording the bin per unit; CTA totals go to pb.partials;
+//      grid barrier;
 //   2. every CTA sums the CTA totals in index order (the grid total, as
 //      grid_reduce forms it) and, with the refinement, picks the threshold
 //      from the histogram (one warp, pick_threshold);
-//   3. with the refinement, each CTA lists the units of its slice at or above
+//   3. with the refinement, each thread lists its unit if it is at or above
 //      the threshold; grid barrier; the listed units are dealt out one per CTA
 //      and re-evaluated by the whole CTA in double-double against the FP64
 //      value the walk computed (rebuilt base, same group evaluator), as
@@ -50,7 +54,7 @@ __host__ __device__ constexpr size_t even(size_t v) { return (v + 1) & ~(size_t)
 // Shared-memory layout, in doubles from the dynamic base; every array
 // starts 16-byte aligned (the evaluators read the table with 16-byte loads).
 struct SmallLayout {
-    size_t a, x0h, x0l, dh, dl, mt, lo, bnd, xw, gw, hist, total;
+    size_t a, x0h, x0l, dh, dl, mt, base, bnd, xw, gw, hist, total;
     __host__ __device__ SmallLayout(int n, int w, int threads)
     {
         const size_t terms = (size_t)1 << w, ntop = n - 1 - w > 0 ? n - 1 - w : 0, nq = terms / 4;
@@ -61,8 +65,8 @@ struct SmallLayout {
         dh = even(x0l + n);
         dl = even(dh + terms * n);
         mt = even(dl + terms * n);
-        lo = even(mt + ntop * n);
-        bnd = even(lo + (size_t)n * threads);
+        base = even(mt + ntop * n);              // [warps][n][33] the walk's unit bases (hi words)
+        bnd = even(base + warps * (size_t)n * 33);
         xw = even(bnd + 2 * (size_t)n);          // [warps][2n] rebuilt unit bases
         gw = even(xw + warps * 2 * (size_t)n);    // [warps][nq] FP64 group sums
         hist = even(gw + warps * nq);             // float[kHistBins] + unsigned[kHistBins]
@@ -124,7 +128,6 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     double* s_dh = smem + L.dh;
     double* s_dl = smem + L.dl;
     double* s_mt = smem + L.mt;
-    double* s_lo = smem + L.lo;
     double* s_bnd = smem + L.bnd;
     float* s_hist = reinterpret_cast<float*>(smem + L.hist);
     unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
@@ -143,12 +146,17 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     if (mode != 0)
         for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
     __syncthreads();
-    for (int r = tid; r < N; r += bd) {
-        double mx = 0.0;
-        for (int j = 0; j < N; ++j) mx = fmax(mx, fabs(s_a[r * N + j]));
-        int e = 0;
-        if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
-        s_exp[r] = e;
+    // row maxima of |a|, a warp per row (fmax does not depend on the order)
+    static_assert(N <= 32, "a row fits a warp");
+    for (int r = wid; r < N; r += bd / 32) {
+        double mx = lane < N ? fabs(s_a[r * N + lane]) : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane == 0) {
+            int e = 0;
+            if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+            s_exp[r] = e;
+        }
     }
     __syncthreads();
     for (int i = tid; i < N * N; i += bd) s_a[i] = ldexp(s_a[i], -s_exp[i / N]);
@@ -200,45 +208,55 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __syncthreads();
     grid.sync();  // the zeroed accumulators are visible before anyone adds to them
 
-    // ---- 1. the walk (walk_real's body on the shared tables)
-    const unsigned long long T = (unsigned long long)gridDim.x * bd;
-    const unsigned long long t = (unsigned long long)blockIdx.x * bd + tid;
-    unsigned long long u0, u1;
-    balanced_range(pb.units, T, t, &u0, &u1);
+    // ---- 1. the walk: one unit per thread (units <= threads: thread t owns
+    // unit t), evaluated as walk_real evaluates it.  The warp builds its 32
+    // unit bases row-parallel: lane r adds the selected high columns of the
+    // warp's first unit to x0_r in ascending order (double-double, as the
+    // refinement rebuilds a base), then takes the 31 Gray steps to the
+    // following units with walk_real's double-double step, storing each hi
+    // word; each lane then reads its own unit's row values.  That is 16 adds
+    // plus 31 steps per row and warp, where building each lane's base alone
+    // costs every lane its own adds for all rows.
+    const unsigned long long u = (unsigned long long)blockIdx.x * bd + tid;
+    const unsigned long long ub = u - (unsigned long long)lane;  // the warp's first unit
+    double* s_base = smem + L.base + (size_t)wid * N * 33;       // [N][33]
+    if (ub < pb.units && lane < N) {
+        const int r = lane;
+        const unsigned long long g = gray_of(ub);
+        dd x = {s_x0h[r], s_x0l[r]};
+        for (int j = 0; j < ntop; ++j)
+            if ((g >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
+        s_base[r * 33] = x.hi;
+        for (int k = 1; k < 32 && ub + k < pb.units; ++k) {
+            const unsigned long long v = ub + k;
+            const int j = __ffsll((long long)v) - 1;
+            const double c = s_mt[j * N + r];
+            const dd sm = two_sum(x.hi, ((gray_of(v) >> j) & 1ull) ? c : -c);
+            x = fast_two_sum(sm.hi, add_rn(sm.lo, x.lo));
+            s_base[r * 33 + k] = x.hi;
+        }
+    }
+    __syncwarp();
     dd tot = {0.0, 0.0};
     HistCache hc;
-    double xh[N];
-    first_base_real<N>(s_x0h, s_x0l, s_mt, s_lo, ntop, u0, u1, tid, bd, xh);
-    if (u0 < u1) {
-        unsigned long long u = u0;
-        while (true) {
-            if (mode == 0) {
-                const double us = unit_sum_real<N, G>(xh, s_dh, nq);
-                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
-            } else {
-                double ub = 1.0;
+    if (u < pb.units) {
+        double xh[N];
 #pragma unroll
-                for (int r = 0; r < N; ++r)
-                    ub = mul_rn(ub, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
-                const int b = hist_bin(ub);
-                pb.raw_b[u] = (unsigned short)b;
-                double sq;
-                const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
-                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
-                hc.add(b, sq, s_hist, s_cnt);
-            }
-            if (++u >= u1) break;
-            const int j = __ffsll((long long)u) - 1;
-            const bool add = (gray_of(u) >> j) & 1ull;
-            const double* col = s_mt + j * N;
+        for (int r = 0; r < N; ++r) xh[r] = s_base[r * 33 + lane];
+        if (mode == 0) {
+            const double us = unit_sum_real<N, G>(xh, s_dh, nq);
+            tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+        } else {
+            double ubd = 1.0;
 #pragma unroll
-            for (int r = 0; r < N; ++r) {
-                const double m = add ? col[r] : -col[r];
-                const dd s = two_sum(xh[r], m);
-                const dd z = fast_two_sum(s.hi, add_rn(s.lo, s_lo[r * bd + tid]));
-                xh[r] = z.hi;
-                s_lo[r * bd + tid] = z.lo;
-            }
+            for (int r = 0; r < N; ++r)
+                ubd = mul_rn(ubd, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
+            const int b = hist_bin(ubd);
+            pb.raw_b[u] = (unsigned short)b;
+            double sq;
+            const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
+            tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+            hc.add(b, sq, s_hist, s_cnt);
         }
     }
     if (mode != 0) {
@@ -280,8 +298,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
 
     // ---- 2. grid total (index order, every CTA alike) and the threshold
     if (wid == 0) {
-        dd v = {0.0, 0.0};
-        for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + b));
+        dd v = lane_sum_dd(pb.partials, (int)gridDim.x, lane);
         v = warp_sum_dd(v);
         if (lane == 0) s_total = v;
         if (mode != 0) {
@@ -308,17 +325,16 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     }
     if (mode == 0 || s_thr >= kHistBins) return;  // nothing to refine (uniform over the grid)
 
-    // ---- 3. refinement of the units at or above the threshold.  Each CTA
-    // lists the units of its slice; after a grid barrier the listed units
+    // ---- 3. refinement of the units at or above the threshold.  Each thread
+    // lists its unit if it qualifies; after a grid barrier the listed units
     // are dealt out one per CTA in list order, so a cluster of dominant units
     // (they gather near the empty and the full subsets) spreads over the grid,
     // and each is refined by a whole CTA.
     const int thr = s_thr;
-    for (unsigned long long u = (unsigned long long)blockIdx.x * bd + tid; u < pb.units; u += T)
-        if ((int)pb.raw_b[u] >= thr) {
-            const unsigned long long k = atomicAdd(pb.list_n, 1ull);
-            if (k < pb.list_cap) pb.list_u[k] = u;
-        }
+    if (u < pb.units && (int)pb.raw_b[u] >= thr) {
+        const unsigned long long k = atomicAdd(pb.list_n, 1ull);
+        if (k < pb.list_cap) pb.list_u[k] = u;
+    }
     grid.sync();
     const unsigned long long listed = __ldcg(pb.list_n);
     const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
@@ -375,8 +391,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __syncthreads();
     if (s_last && wid == 0) {
         __threadfence();
-        dd v = {0.0, 0.0};
-        for (int b = lane; b < (int)gridDim.x; b += 32) v = dd_add(v, ldcg_dd(pb.partials + gridDim.x + b));
+        dd v = lane_sum_dd(pb.partials + gridDim.x, (int)gridDim.x, lane);
         v = warp_sum_dd(v);
         if (lane == 0) {
             pb.rb->corr[0] = v;
