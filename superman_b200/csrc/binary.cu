@@ -95,26 +95,26 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
     if (blocks < 1) blocks = 1;
     pb.grid = blocks;
-    const size_t smem = sizeof(float) * ((size_t)terms * n + (size_t)(ntop > 0 ? ntop : 1) * n);
+    const size_t smem = sizeof(int) * terms * n + align_up((size_t)(ntop > 0 ? ntop : 1) * n, 16);
 
-    // host-built tables (small integers, exact as floats): x'_r = 2 a_{r,n-1}
-    // - rowsum_r, doubled low-column counts, doubled high columns
-    std::vector<float> x0(n);
+    // host-built tables: x'_r = 2 a_{r,n-1} - rowsum_r, doubled low-column
+    // counts, doubled high columns
+    std::vector<int> x0(n);
     for (int r = 0; r < n; ++r) {
         int rs = 0;
         for (int j = 0; j < n; ++j) rs += a[r * n + j] ? 1 : 0;
-        x0[r] = (float)(2 * (a[r * n + n - 1] ? 1 : 0) - rs);
+        x0[r] = 2 * (a[r * n + n - 1] ? 1 : 0) - rs;
     }
-    std::vector<float> dei((size_t)terms * n);
+    std::vector<int> dei((size_t)terms * n);
     for (int d = 0; d < terms; ++d)
         for (int r = 0; r < n; ++r) {
             int c = 0;
             for (int j = 0; j < w; ++j) c += ((d >> j) & 1) && a[r * n + j] ? 2 : 0;
-            dei[((size_t)(d / 4) * n + r) * 4 + (d % 4)] = (float)c;
+            dei[((size_t)(d / 4) * n + r) * 4 + (d % 4)] = c;
         }
-    std::vector<float> mt((size_t)(ntop > 0 ? ntop : 1) * n, 0.0f);
+    std::vector<int8_t> mt((size_t)(ntop > 0 ? ntop : 1) * n, 0);
     for (int j = 0; j < ntop; ++j)
-        for (int r = 0; r < n; ++r) mt[(size_t)j * n + r] = a[r * n + w + j] ? 2.0f : 0.0f;
+        for (int r = 0; r < n; ++r) mt[(size_t)j * n + r] = a[r * n + w + j] ? 2 : 0;
 
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -122,25 +122,25 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
         off = align_up(off + bytes, 256);
         return o;
     };
-    const size_t o_x0 = take(sizeof(float) * n);
-    const size_t o_de = take(sizeof(float) * dei.size());
-    const size_t o_mt = take(sizeof(float) * mt.size());
+    const size_t o_x0 = take(sizeof(int) * n);
+    const size_t o_de = take(sizeof(int) * dei.size());
+    const size_t o_mt = take(mt.size());
     const size_t o_part = take(sizeof(uint32_t) * kMaxLimbs * blocks);
     const size_t o_tick = take(sizeof(unsigned) * 4);
     const size_t o_res = take(sizeof(uint32_t) * kMaxLimbs);
     if ((st = ensure_scratch(ctx, off)) != SPB_OK) return out->status = st;
     char* base = static_cast<char*>(ctx->scratch);
-    pb.x0 = reinterpret_cast<const float*>(base + o_x0);
-    pb.dei = reinterpret_cast<const float*>(base + o_de);
-    pb.mt = reinterpret_cast<const float*>(base + o_mt);
+    pb.x0 = reinterpret_cast<const int*>(base + o_x0);
+    pb.dei = reinterpret_cast<const int*>(base + o_de);
+    pb.mt = reinterpret_cast<const int8_t*>(base + o_mt);
     pb.partials = reinterpret_cast<uint32_t*>(base + o_part);
     pb.ticket = reinterpret_cast<unsigned*>(base + o_tick);
     pb.result = reinterpret_cast<uint32_t*>(base + o_res);
 
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
-    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_x0, x0.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream));
-    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_de, dei.data(), sizeof(float) * dei.size(), cudaMemcpyHostToDevice, stream));
-    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_mt, mt.data(), sizeof(float) * mt.size(), cudaMemcpyHostToDevice, stream));
+    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_x0, x0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_de, dei.data(), sizeof(int) * dei.size(), cudaMemcpyHostToDevice, stream));
+    SPB_CUDA_TRY(cudaMemcpyAsync(base + o_mt, mt.data(), mt.size(), cudaMemcpyHostToDevice, stream));
     SPB_CUDA_TRY(cudaMemsetAsync(pb.ticket, 0, sizeof(unsigned) * 4, stream));
     SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
     if ((st = launch_binary(pb, blocks, threads, smem, stream)) != SPB_OK) return out->status = st;
