@@ -17,10 +17,12 @@
 // columns of d (grouped [d/4][r][d%4], so one 16-byte broadcast load serves
 // four terms); the n-1-w high columns form a unit index walked in Gray order
 // per thread with the integer unit base xtop_r in registers.  Each term
-// multiplies up to K row values in signed 32-bit arithmetic (n^K < 2^31, so
-// exact), folds the magnitudes into L 32-bit limbs with 32x32->64
-// multiply-adds and applies the sign once.  Unit sums and the grid reduction
-// are exact, so the result does not depend on the launch shape.
+// multiplies its row values in words of up to K rows (n^K < 2^32: the word's
+// magnitude is an exact unsigned 32-bit integer), folds the word magnitudes
+// into L 32-bit limbs with 32x32->64 multiply-adds over only the limbs the
+// bit widths so far can reach, and applies the sign (the xor of the words')
+// once.  Unit sums and the grid reduction are exact, so the result does not
+// depend on the launch shape.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,32 +47,44 @@ struct Problem {
     uint32_t* result;          // [limbs] sum over subsets, mod 2^(32*limbs)
 };
 
-// Rows per signed 32-bit partial product: largest K with N^K < 2^31
-// (|x'_r| <= N, so the product is exact).
+// Rows per word: the largest K with n^K < 2^32, so a word's magnitude fits
+// an unsigned 32-bit integer (|x'_r| <= n).  Its first K-1 rows multiply in
+// signed 32-bit arithmetic (n^(K-1) < 2^31: exact); the last row's magnitude
+// multiplies the magnitude of that product, unsigned.
 __host__ __device__ constexpr int rows_per_word(int n)
 {
     int k = 1;
     const unsigned long long b = (unsigned long long)(n > 1 ? n : 2);
     unsigned long long p = b;
-    while (p * b < (1ull << 31) && k < 16) {
+    while (p * b < (1ull << 32) && k < 16) {
         p *= b;
         ++k;
     }
     return k;
 }
 
-// a += p, or a -= p when sub, modulo 2^(32L): a + (p xor mask) + sub.
-template <int L>
-__device__ __forceinline__ void limb_add_signed(uint32_t (&a)[L], const uint32_t (&p)[L], bool sub)
+// Bit width of n^k, the largest magnitude of a word of k rows.
+__host__ __device__ constexpr int word_bits(int n, int k)
 {
-    const uint32_t mask = sub ? 0xffffffffu : 0u;
-    uint64_t c = sub ? 1u : 0u;
-#pragma unroll
-    for (int i = 0; i < L; ++i) {
-        uint64_t t = (uint64_t)a[i] + (p[i] ^ mask) + c;
-        a[i] = (uint32_t)t;
-        c = t >> 32;
+    unsigned long long p = 1;
+    for (int i = 0; i < k; ++i) p *= (unsigned long long)n;
+    int b = 0;
+    while (b < 63 && (1ull << b) <= p) ++b;
+    return b;
+}
+
+// Limbs that can be nonzero in the product of words 0..g (at most L): the
+// bit widths of the words so far, summed, in 32-bit limbs.
+__host__ __device__ constexpr int limbs_after(int n, int g, int L)
+{
+    const int K = rows_per_word(n);
+    int bits = 0;
+    for (int h = 0; h <= g; ++h) {
+        const int rows = n - h * K < K ? n - h * K : K;
+        bits += word_bits(n, rows);
     }
+    const int l = (bits + 31) / 32;
+    return l < L ? l : L;
 }
 
 template <int L>
@@ -97,42 +111,69 @@ __device__ __forceinline__ void limb_sub(uint32_t (&a)[L], const uint32_t (&b)[L
     }
 }
 
-// prod_r x'_r mod 2^(32L) for one term; x'_r = xt[r] + de(r), signed.
+// |prod_r x'_r| mod 2^(32L) for one term (x'_r = xt[r] + de(r), signed) into
+// p; returns a word whose bit 31 is the product's sign (the xor of the
+// factors' signs).  Per word: the signed product of its first rows, then the
+// unsigned product of the magnitudes with its last row; the word magnitudes
+// multiply into the limbs that the bit widths so far can reach, the carry out
+// of the top one landing in the next (dropped past L: mod 2^(32L)).
 template <int N, int L, int G>
-__device__ __forceinline__ bool term_product(const int (&xt)[N], const int* __restrict__ de, int i,
-                                             uint32_t (&p)[L])
+__device__ __forceinline__ uint32_t term_product(const int (&xt)[N], const int* __restrict__ de, int i,
+                                                 uint32_t (&p)[L])
 {
     constexpr int K = rows_per_word(N);
     constexpr int NG = (N + K - 1) / K;
 #pragma unroll
     for (int l = 0; l < L; ++l) p[l] = 0u;
-    bool neg = false;
+    uint32_t sg = 0u;
 #pragma unroll
     for (int g = 0; g < NG; ++g) {
-        int sw = 1;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int r = g * K + k;
-            if (r < N) sw *= xt[r] + de[r * G + i];
-        }
-        neg ^= sw < 0;
-        const uint32_t w = (uint32_t)(sw < 0 ? -sw : sw);
-        if (g == 0) {
-            p[0] = w;
+        const int r0 = g * K, rows = N - r0 < K ? N - r0 : K;
+        uint32_t m;
+        if (rows == 1) {
+            const int x = xt[r0] + de[r0 * G + i];
+            sg ^= (uint32_t)x;
+            m = (uint32_t)(x < 0 ? -x : x);
         } else {
-            // p *= w, only the limbs that can be nonzero after g words
+            int sw = xt[r0] + de[r0 * G + i];
+#pragma unroll
+            for (int k = 1; k < K - 1; ++k)
+                if (k < rows - 1) sw *= xt[r0 + k] + de[(r0 + k) * G + i];
+            const int x = xt[r0 + rows - 1] + de[(r0 + rows - 1) * G + i];
+            sg ^= (uint32_t)sw ^ (uint32_t)x;
+            m = (uint32_t)(sw < 0 ? -sw : sw) * (uint32_t)(x < 0 ? -x : x);
+        }
+        if (g == 0) {
+            p[0] = m;
+        } else {
+            const int nb = limbs_after(N, g - 1, L);
             uint64_t c = 0;
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-                if (l <= g) {
-                    uint64_t t = (uint64_t)p[l] * w + c;
+            for (int l = 0; l < L; ++l)
+                if (l < nb) {
+                    const uint64_t t = (uint64_t)p[l] * m + c;
                     p[l] = (uint32_t)t;
                     c = t >> 32;
                 }
-            }
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (l == nb) p[l] = (uint32_t)c;
         }
     }
-    return neg;  // the term is -p when set
+    return sg;
+}
+
+// a += p when mask is 0, a -= p when mask is all ones, modulo 2^(32L).
+template <int L>
+__device__ __forceinline__ void limb_add_masked(uint32_t (&a)[L], const uint32_t (&p)[L], uint32_t mask)
+{
+    uint64_t c = mask & 1u;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const uint64_t t = (uint64_t)a[l] + (p[l] ^ mask) + c;
+        a[l] = (uint32_t)t;
+        c = t >> 32;
+    }
 }
 
 // Sum over one unit: sum_d (-1)^popc(d) prod_r (xt_r + DEI[d][r]).
@@ -146,18 +187,18 @@ __device__ __forceinline__ void unit_sum_bin(const int (&xt)[N], const int* __re
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
         const int* de = s_de + q * (N * G);
-        // group signs relative to popc(q): + - - +; each term also carries
-        // the sign of its product
-        const bool odd = __popc(q) & 1;
+        // signs: the product's (bit 31 of the returned word) and the group
+        // pattern + - - + relative to popc(q); an all-ones mask subtracts
+        const uint32_t flip = (__popc(q) & 1) ? 0x80000000u : 0u;
         uint32_t p[L];
-        bool neg = term_product<N, L, G>(xt, de, 0, p);
-        limb_add_signed<L>(acc, p, neg != odd);
-        neg = term_product<N, L, G>(xt, de, 1, p);
-        limb_add_signed<L>(acc, p, neg == odd);
-        neg = term_product<N, L, G>(xt, de, 2, p);
-        limb_add_signed<L>(acc, p, neg == odd);
-        neg = term_product<N, L, G>(xt, de, 3, p);
-        limb_add_signed<L>(acc, p, neg != odd);
+        uint32_t sg = term_product<N, L, G>(xt, de, 0, p);
+        limb_add_masked<L>(acc, p, (uint32_t)((int32_t)(sg ^ flip) >> 31));
+        sg = term_product<N, L, G>(xt, de, 1, p);
+        limb_add_masked<L>(acc, p, (uint32_t)((int32_t)(sg ^ flip ^ 0x80000000u) >> 31));
+        sg = term_product<N, L, G>(xt, de, 2, p);
+        limb_add_masked<L>(acc, p, (uint32_t)((int32_t)(sg ^ flip ^ 0x80000000u) >> 31));
+        sg = term_product<N, L, G>(xt, de, 3, p);
+        limb_add_masked<L>(acc, p, (uint32_t)((int32_t)(sg ^ flip) >> 31));
     }
 }
 

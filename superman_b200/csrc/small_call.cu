@@ -24,9 +24,10 @@
 //      from the histogram (one warp, pick_threshold);
 //   3. with the refinement, each thread lists its unit if it is at or above
 //      the threshold; grid barrier; the listed units are dealt out one per CTA
-//      and re-evaluated by the whole CTA in double-double against the FP64
-//      value the walk computed (rebuilt base, same group evaluator), as
-//      refine_real does; the last CTA sums the corrections in index order.
+//      and re-evaluated by the whole CTA in double-double (base rebuilt from
+//      x0 and the high columns, as refine_real does), against the FP64 value
+//      the walk stored for the unit; the last CTA sums the corrections in
+//      index order.
 // The last CTA to finish copies the readback into page-locked host memory
 // mapped into the device's address space, so the host copies nothing after
 // the kernel.  Nothing waits on anything but the grid barriers of
@@ -54,10 +55,10 @@ __host__ __device__ constexpr size_t even(size_t v) { return (v + 1) & ~(size_t)
 // Shared-memory layout, in doubles from the dynamic base; every array
 // starts 16-byte aligned (the evaluators read the table with 16-byte loads).
 struct SmallLayout {
-    size_t a, x0h, x0l, dh, dl, mt, base, bnd, xw, gw, hist, total;
+    size_t a, x0h, x0l, dh, dl, mt, base, bnd, xw, hist, total;
     __host__ __device__ SmallLayout(int n, int w, int threads)
     {
-        const size_t terms = (size_t)1 << w, ntop = n - 1 - w > 0 ? n - 1 - w : 0, nq = terms / 4;
+        const size_t terms = (size_t)1 << w, ntop = n - 1 - w > 0 ? n - 1 - w : 0;
         const size_t warps = threads / 32;
         a = 0;
         x0h = even(a + (size_t)n * n);
@@ -67,9 +68,8 @@ struct SmallLayout {
         mt = even(dl + terms * n);
         base = even(mt + ntop * n);              // [warps][n][33] the walk's unit bases (hi words)
         bnd = even(base + warps * (size_t)n * 33);
-        xw = even(bnd + 2 * (size_t)n);          // [warps][2n] rebuilt unit bases
-        gw = even(xw + warps * 2 * (size_t)n);    // [warps][nq] FP64 group sums
-        hist = even(gw + warps * nq);             // float[kHistBins] + unsigned[kHistBins]
+        xw = even(bnd + 2 * (size_t)n);          // [2n] the refined unit's base, hi then lo
+        hist = even(xw + 2 * (size_t)n);          // float[kHistBins] + unsigned[kHistBins]
         total = hist + (kHistSmemBytes + sizeof(double) - 1) / sizeof(double);
     }
     size_t bytes() const { return total * sizeof(double); }
@@ -103,6 +103,11 @@ __device__ __forceinline__ void publish(const Problem& pb, Readback* host)
     for (int i = 0; i < (int)(sizeof(Readback) / sizeof(unsigned long long)); ++i) dst[i] = __ldcg(src + i);
 }
 static_assert(sizeof(Readback) % sizeof(unsigned long long) == 0, "readback copied in 8-byte words");
+
+// The walk's FP64 value of each unit, kept for the refinement in the space
+// of the separate kernels' unit list (pb.raw_u, kRawCap entries of 8 bytes,
+// unused by this call; units <= kRawCap here).
+__device__ __forceinline__ double* unit_value(const Problem& pb) { return reinterpret_cast<double*>(pb.raw_u); }
 
 template <int N>
 __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* __restrict__ a_in,
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __syncthreads();
     for (int i = tid; i < N * N; i += bd) s_a[i] = ldexp(s_a[i], -s_exp[i / N]);
     __syncthreads();
-    if (blockIdx.x == 0 && tid == 0) {
+    if (blockIdx.x == 0 && tid == bd - 1) {  // not a row thread (bd >= 32 > N): the x0 sums start at once
         int es = 0;
         for (int r = 0; r < N; ++r) es += s_exp[r];
         *pb.exp_sum = es;
@@ -257,6 +262,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
             const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
             tot = dd_add_d(tot, (u & 1ull) ? -us : us);
             hc.add(b, sq, s_hist, s_cnt);
+            unit_value(pb)[u] = us;  // what the refinement corrects
         }
     }
     if (mode != 0) {
@@ -339,7 +345,6 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     const unsigned long long listed = __ldcg(pb.list_n);
     const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
     double* xw = smem + L.xw;  // [2N]: the unit base, hi then lo
-    double* gw = smem + L.gw;  // [nq]: the walk's FP64 group sums
     // threads per term: a power of two up to a warp (so a term's threads are
     // lanes of one warp and every warp's terms are all in range or all out),
     // as many as the CTA holds for all terms at once; each takes a run of rows
@@ -360,8 +365,6 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
             xw[N + r] = x.lo;
         }
         __syncthreads();
-        // the unit's FP64 value exactly as the walk computed it, group by group
-        for (int q = tid; q < nq; q += bd) gw[q] = group_sum_real_rt(xw, s_dh + q * (N * G), N, N, G, G);
         // its double-double value: each term's product over the rows of
         // `per` threads, joined by shuffles
         dd acc = {0.0, 0.0};
@@ -372,15 +375,14 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
             for (int off = 1; off < per; off <<= 1) p = dd_mul(p, shfl_xor_dd(p, off));
             if (sub == 0) acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
         }
-        acc = block_sum_dd(acc, s_warp);  // also orders gw's writes before thread 0 reads them
+        acc = block_sum_dd(acc, s_warp);
         if (tid == 0) {
-            double f = 0.0;
-            for (int q = 0; q < nq; ++q) f = (__popc(q) & 1) ? sub_rn(f, gw[q]) : add_rn(f, gw[q]);
-            dd c = dd_add_d(acc, -f);
+            // against the value the walk added for this unit
+            dd c = dd_add_d(acc, -__ldcg(unit_value(pb) + u));
             if (u & 1ull) c = dd_neg(c);
             corr = dd_add(corr, c);
         }
-        __syncthreads();  // xw and gw are rewritten by the next unit
+        __syncthreads();  // xw is rewritten by the next unit
     }
     if (tid == 0) {
         pb.partials[gridDim.x + blockIdx.x] = corr;
