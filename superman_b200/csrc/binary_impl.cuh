@@ -111,55 +111,59 @@ __device__ __forceinline__ void limb_sub(uint32_t (&a)[L], const uint32_t (&b)[L
     }
 }
 
+// Word g of a term (rows g*K .. g*K + rows - 1): the signed product of its
+// first rows, then the unsigned product of the magnitudes with its last row;
+// its sign bit is xor-ed into sg and its magnitude multiplied into the limbs
+// that the bit widths of words 0..g-1 can reach (a compile-time count), the
+// carry out of the top one landing in the next (dropped past L: mod 2^(32L)).
+// Recurses over g so that every count is a constant.
+template <int N, int L, int G, int g>
+__device__ __forceinline__ void term_word(const int (&xt)[N], const int* __restrict__ de, int i,
+                                          uint32_t (&p)[L], uint32_t& sg)
+{
+    constexpr int K = rows_per_word(N);
+    constexpr int NG = (N + K - 1) / K;
+    constexpr int r0 = g * K, rows = N - r0 < K ? N - r0 : K;
+    uint32_t m;
+    if constexpr (rows == 1) {
+        const int x = xt[r0] + de[r0 * G + i];
+        sg ^= (uint32_t)x;
+        m = (uint32_t)(x < 0 ? -x : x);
+    } else {
+        int sw = xt[r0] + de[r0 * G + i];
+#pragma unroll
+        for (int k = 1; k < rows - 1; ++k) sw *= xt[r0 + k] + de[(r0 + k) * G + i];
+        const int x = xt[r0 + rows - 1] + de[(r0 + rows - 1) * G + i];
+        sg ^= (uint32_t)sw ^ (uint32_t)x;
+        m = (uint32_t)(sw < 0 ? -sw : sw) * (uint32_t)(x < 0 ? -x : x);
+    }
+    if constexpr (g == 0) {
+        p[0] = m;
+    } else {
+        constexpr int nb = limbs_after(N, g - 1, L);
+        uint64_t c = 0;
+#pragma unroll
+        for (int l = 0; l < nb; ++l) {
+            const uint64_t t = (uint64_t)p[l] * m + c;
+            p[l] = (uint32_t)t;
+            c = t >> 32;
+        }
+        if constexpr (nb < L) p[nb] = (uint32_t)c;
+    }
+    if constexpr (g + 1 < NG) term_word<N, L, G, g + 1>(xt, de, i, p, sg);
+}
+
 // |prod_r x'_r| mod 2^(32L) for one term (x'_r = xt[r] + de(r), signed) into
 // p; returns a word whose bit 31 is the product's sign (the xor of the
-// factors' signs).  Per word: the signed product of its first rows, then the
-// unsigned product of the magnitudes with its last row; the word magnitudes
-// multiply into the limbs that the bit widths so far can reach, the carry out
-// of the top one landing in the next (dropped past L: mod 2^(32L)).
+// factors' signs).
 template <int N, int L, int G>
 __device__ __forceinline__ uint32_t term_product(const int (&xt)[N], const int* __restrict__ de, int i,
                                                  uint32_t (&p)[L])
 {
-    constexpr int K = rows_per_word(N);
-    constexpr int NG = (N + K - 1) / K;
 #pragma unroll
     for (int l = 0; l < L; ++l) p[l] = 0u;
     uint32_t sg = 0u;
-#pragma unroll
-    for (int g = 0; g < NG; ++g) {
-        const int r0 = g * K, rows = N - r0 < K ? N - r0 : K;
-        uint32_t m;
-        if (rows == 1) {
-            const int x = xt[r0] + de[r0 * G + i];
-            sg ^= (uint32_t)x;
-            m = (uint32_t)(x < 0 ? -x : x);
-        } else {
-            int sw = xt[r0] + de[r0 * G + i];
-#pragma unroll
-            for (int k = 1; k < K - 1; ++k)
-                if (k < rows - 1) sw *= xt[r0 + k] + de[(r0 + k) * G + i];
-            const int x = xt[r0 + rows - 1] + de[(r0 + rows - 1) * G + i];
-            sg ^= (uint32_t)sw ^ (uint32_t)x;
-            m = (uint32_t)(sw < 0 ? -sw : sw) * (uint32_t)(x < 0 ? -x : x);
-        }
-        if (g == 0) {
-            p[0] = m;
-        } else {
-            const int nb = limbs_after(N, g - 1, L);
-            uint64_t c = 0;
-#pragma unroll
-            for (int l = 0; l < L; ++l)
-                if (l < nb) {
-                    const uint64_t t = (uint64_t)p[l] * m + c;
-                    p[l] = (uint32_t)t;
-                    c = t >> 32;
-                }
-#pragma unroll
-            for (int l = 0; l < L; ++l)
-                if (l == nb) p[l] = (uint32_t)c;
-        }
-    }
+    term_word<N, L, G, 0>(xt, de, i, p, sg);
     return sg;
 }
 

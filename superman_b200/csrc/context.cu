@@ -122,6 +122,7 @@ void destroy_context(DeviceContext* ctx)
     if (!ctx) return;
     if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->release_small_graphs) ctx->release_small_graphs(ctx->small_graphs);
     for (cudaEvent_t ev : {ctx->ev_begin, ctx->ev_end, ctx->ev_call0, ctx->ev_call1, ctx->ev_ref0, ctx->ev_ref1})
         if (ev) cudaEventDestroy(ev);
     if (ctx->scratch) cudaFree(ctx->scratch);

@@ -26,6 +26,10 @@ struct DeviceContext {
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     void* pinned_dev = nullptr;  // the device's address of `pinned` (null if it has none)
+    // CUDA graphs of the fused small call, cached per launch (small_call.cu
+    // owns the cache; destroy_context frees it through release_small_graphs).
+    void* small_graphs = nullptr;
+    void (*release_small_graphs)(void*) = nullptr;
     std::mutex mu;  // serialises calls that use this context
 };
 

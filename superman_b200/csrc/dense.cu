@@ -188,6 +188,9 @@ constexpr int kSmallCallMaxN = 24;
 size_t small_call_smem_bytes(int n, int w, int threads);
 int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, Readback* rb_host, int dev,
                       int sms, cudaStream_t s, bool* launched);
+int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* stage,
+                            size_t a_bytes, int blocks, int threads, Readback* rb_host, cudaStream_t s,
+                            bool* launched);
 
 // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
 // subset-sum table: the setup kernel's dynamic shared-memory limit is raised to
@@ -419,7 +422,12 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     if ((st = ensure_scratch(ctx, need)) != SPB_OK) return out->status = st;
     char* base = static_cast<char*>(ctx->scratch);
     plan_layout(&pb, base, &in_off);
-    if ((st = ensure_pinned(ctx, sizeof(Readback))) != SPB_OK) return out->status = st;
+    // page-locked: the readback, then (fused small call) a staging copy of a
+    // host matrix
+    constexpr size_t kStageOff = 256;
+    static_assert(sizeof(Readback) <= kStageOff, "readback fits before the staging area");
+    const size_t a_bytes = sizeof(double) * n * n * comps;
+    if ((st = ensure_pinned(ctx, kStageOff + a_bytes)) != SPB_OK) return out->status = st;
     Readback* hrb = static_cast<Readback*>(ctx->pinned);
     // The refinement list is sized before the walk for the threshold's cap
     // (1/8 of the units), up to 2^21 units; a larger count is met after the
@@ -433,26 +441,36 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         pb.list_x = nullptr;
         pb.tol = opt.rel_tol > 0.0 ? opt.rel_tol : 1e-13;
     }
-    SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
-    const double* d_a = a;
-    if (!a_on_device) {
-        double* d_in = reinterpret_cast<double*>(base + in_off);
-        SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, sizeof(double) * n * n * comps,
-                                     cudaMemcpyHostToDevice, stream));
-        d_a = d_in;
-    }
+    double* d_in = reinterpret_cast<double*>(base + in_off);
+    const double* d_a = a_on_device ? a : d_in;
     dd res[2] = {{0.0, 0.0}, {0.0, 0.0}};
     int exp_sum = 0, launches = 0;
     double ms_refine = 0.0;
     // Small real matrices: the whole call as one cooperative kernel
     // (small_call.cu), unless the device cannot hold its grid or its count
-    // check fails, in which case the separate kernels below run.
-    bool fused = false;
-    if (small_candidate && pb.units <= (unsigned long long)blocks * threads && pb.units <= kRawCap &&
-        small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin) {
-        // The kernel writes the finished readback straight into the pinned
-        // buffer when the device can address it (no copy after the kernel).
-        Readback* mapped = static_cast<Readback*>(ctx->pinned_dev);
+    // check fails, in which case the separate kernels below run.  The kernel
+    // writes the finished readback straight into the pinned buffer when the
+    // device can address it (no copy after the kernel).  A launch asked for
+    // again is replayed as a CUDA graph (events, matrix copy from the
+    // pinned staging area, kernel): one graph launch instead of ~10 us of
+    // host calls during which the device waits.
+    const bool fused_fits = small_candidate && pb.units <= (unsigned long long)blocks * threads &&
+                            pb.units <= kRawCap && small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin;
+    Readback* mapped = static_cast<Readback*>(ctx->pinned_dev);
+    bool fused = false, staged = false;
+    if (fused_fits && mapped) {
+        double* stage = reinterpret_cast<double*>(static_cast<char*>(ctx->pinned) + kStageOff);
+        if (!a_on_device) std::memcpy(stage, a, a_bytes);
+        if ((st = launch_small_call_graph(ctx, pb, d_a, a_on_device ? nullptr : stage, a_bytes, blocks, threads,
+                                          mapped, stream, &fused)) != SPB_OK)
+            return out->status = st;
+        staged = fused;
+    }
+    if (!staged) {
+        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
+        if (!a_on_device) SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, a_bytes, cudaMemcpyHostToDevice, stream));
+    }
+    if (fused_fits && !staged) {
         SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
         if ((st = launch_small_call(pb, d_a, blocks, threads, mapped, ctx->device, ctx->sm_count, stream,
                                     &fused)) != SPB_OK)
@@ -460,17 +478,18 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         if (fused) {
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
             SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
-            if (!mapped)
-                SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
-            SPB_CUDA_TRY(cudaStreamSynchronize(stream));
-            launches = 1;
-            res[0] = dd_add(hrb->res[0], hrb->corr[0]);
-            exp_sum = hrb->exp_sum;
-            if (dd_mode) {
-                out->err_est = hrb->err;
-                out->refined_units = hrb->count;
-                if (hrb->list_n != hrb->count) fused = false;  // run the separate kernels instead
-            }
+        }
+    }
+    if (fused) {
+        if (!mapped) SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
+        SPB_CUDA_TRY(cudaStreamSynchronize(stream));
+        launches = 1;
+        res[0] = dd_add(hrb->res[0], hrb->corr[0]);
+        exp_sum = hrb->exp_sum;
+        if (dd_mode) {
+            out->err_est = hrb->err;
+            out->refined_units = hrb->count;
+            if (hrb->list_n != hrb->count) fused = false;  // run the separate kernels instead
         }
     }
     if (!fused) {

@@ -35,8 +35,10 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <mutex>
 
+#include "context.h"
 #include "dense_impl.cuh"
 #include "refine_impl.cuh"
 
@@ -423,6 +425,44 @@ SmallKernel small_kernel(int n)
 
 size_t small_call_smem_bytes(int n, int w, int threads) { return SmallLayout(n, w, threads).bytes(); }
 
+// Whether the fused call can run on device `dev` (the current one, with
+// `sms` SMs) with `blocks` CTAs of `threads` threads all resident at once
+// (one CTA per SM); configures the kernel's shared memory on first use.
+// Asked once per device, size and shape.
+static int small_call_ready(SmallKernel kern, const Problem& pb, int blocks, int threads, int dev, int sms,
+                            size_t smem, bool* ok)
+{
+    *ok = false;
+    if (!kern || threads > kSmallCallThreads || threads < 32 || threads % 32 != 0) return SPB_OK;
+    if (dev < 0 || dev >= 64 || blocks > sms) return SPB_OK;  // one CTA per SM must hold the whole grid
+    static std::mutex mu;
+    static int fits[64][kSmallCallMaxN + 1];  // 0 unknown, 1 kernel configured, -1 cannot run
+    static signed char resident[64][kSmallCallMaxN + 1][kSmallCallThreads / 32 + 1];  // 0 unknown, 1, -1
+    std::lock_guard<std::mutex> lk(mu);
+    if (fits[dev][pb.n] == 0) {
+        int optin = 0, coop = 0;
+        cudaFuncAttributes fa{};
+        SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        SPB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+        fits[dev][pb.n] = -1;
+        if (coop) {
+            SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              optin - (int)fa.sharedSizeBytes));
+            fits[dev][pb.n] = 1;
+        }
+    }
+    if (fits[dev][pb.n] < 0) return SPB_OK;
+    signed char& res = resident[dev][pb.n][threads / 32];
+    if (res == 0) {
+        int per_sm = 0;
+        SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+        res = per_sm >= 1 ? 1 : -1;
+    }
+    *ok = res > 0;
+    return SPB_OK;
+}
+
 // Launches the fused call on device `dev` (the current one, with `sms`
 // SMs) if it can keep `blocks` CTAs of `threads` threads resident at once;
 // *launched tells whether it did.  rb_host (may be null): the device's
@@ -432,43 +472,159 @@ int launch_small_call(const Problem& pb, const double* d_a, int blocks, int thre
 {
     *launched = false;
     SmallKernel kern = small_kernel(pb.n);
-    if (!kern || threads > kSmallCallThreads || threads < 32 || threads % 32 != 0) return SPB_OK;
-    if (dev < 0 || dev >= 64 || blocks > sms) return SPB_OK;  // one CTA per SM must hold the whole grid
     const size_t smem = small_call_smem_bytes(pb.n, pb.w, threads);
-    static std::mutex mu;
-    static int fits[64][kSmallCallMaxN + 1];  // 0 unknown, 1 kernel configured, -1 cannot run
-    static signed char resident[64][kSmallCallMaxN + 1][kSmallCallThreads / 32 + 1];  // 0 unknown, 1, -1
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (fits[dev][pb.n] == 0) {
-            int optin = 0, coop = 0;
-            cudaFuncAttributes fa{};
-            SPB_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            SPB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-            SPB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
-            fits[dev][pb.n] = -1;
-            if (coop) {
-                SPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  optin - (int)fa.sharedSizeBytes));
-                fits[dev][pb.n] = 1;
-            }
-        }
-        if (fits[dev][pb.n] < 0) return SPB_OK;
-        // one CTA of this shape must fit an SM (shared memory, registers);
-        // asked once per device, size and shape
-        signed char& res = resident[dev][pb.n][threads / 32];
-        if (res == 0) {
-            int per_sm = 0;
-            SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-            res = per_sm >= 1 ? 1 : -1;
-        }
-        if (res < 0) return SPB_OK;
-    }
+    bool ok = false;
+    int st = small_call_ready(kern, pb, blocks, threads, dev, sms, smem, &ok);
+    if (st != SPB_OK || !ok) return st;
     Problem p = pb;
     const double* a = d_a;
     Readback* h = rb_host;
     void* args[] = {&p, &a, &h};
     SPB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(blocks), dim3(threads), args, smem, s));
+    *launched = true;
+    return SPB_OK;
+}
+
+// ---- the call as a CUDA graph --------------------------------------------
+// A call issues the events around it, the matrix copy and the cooperative
+// launch: about 10 us of host time, during which the device waits for the
+// launch.  Replayed as one graph (events, copy from the context's page-locked
+// staging, kernel) it costs one graph launch.  A graph is built for a launch
+// (the kernel's Problem, its matrix and readback addresses, the shape) the
+// second time that launch is asked for in a row of calls, and kept in a small
+// per-context cache; a matrix given on the device is part of the launch, so
+// a caller that passes a new device pointer each time keeps the direct path.
+namespace {
+
+struct SmallGraph {
+    bool valid = false;         // the key below is set
+    bool failed = false;        // building the graph failed: use the direct path
+    int uses = 0;
+    unsigned long long stamp = 0;
+    Problem pb{};
+    const double* a = nullptr;  // the matrix the kernel reads
+    const double* stage = nullptr;  // page-locked source of the matrix copy (host input) or null
+    size_t a_bytes = 0;
+    Readback* rb_host = nullptr;
+    int blocks = 0, threads = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+struct SmallGraphCache {
+    SmallGraph e[8];
+    unsigned long long clock = 0;
+};
+
+void drop(SmallGraph& g)
+{
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = SmallGraph{};
+}
+
+void release_cache(void* p)
+{
+    SmallGraphCache* c = static_cast<SmallGraphCache*>(p);
+    if (!c) return;
+    for (SmallGraph& g : c->e) drop(g);
+    delete c;
+}
+
+bool same_launch(const SmallGraph& g, const Problem& pb, const double* a, const double* stage, size_t a_bytes,
+                 Readback* rb_host, int blocks, int threads)
+{
+    return g.valid && std::memcmp(&g.pb, &pb, sizeof(Problem)) == 0 && g.a == a && g.stage == stage &&
+           g.a_bytes == a_bytes && g.rb_host == rb_host && g.blocks == blocks && g.threads == threads;
+}
+
+// Captures events, copy and kernel on the context's own stream.  Any error
+// ends the capture and leaves the entry marked failed.
+void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
+{
+    cudaStream_t cs = ctx->stream;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        g.failed = true;
+        return;
+    }
+    Problem p = g.pb;
+    const double* a = g.a;
+    Readback* h = g.rb_host;
+    void* args[] = {&p, &a, &h};
+    cudaError_t e = cudaEventRecordWithFlags(ctx->ev_call0, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess && g.stage)
+        e = cudaMemcpyAsync(const_cast<double*>(g.a), g.stage, g.a_bytes, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_begin, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess)
+        e = cudaLaunchCooperativeKernel((const void*)kern, dim3(g.blocks), dim3(g.threads), args, smem, cs);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_end, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_call1, cs, cudaEventRecordExternal);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+    g.graph = graph;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        g.exec = nullptr;
+        g.graph = nullptr;
+        g.failed = true;
+    }
+}
+
+}  // namespace
+
+// The fused call through a cached graph, on stream s.  The kernel reads its
+// matrix at d_a; with host input, stage (page-locked, holding the matrix)
+// is copied there first, inside the graph.  The graph also records the
+// context's events ev_call0, ev_begin, ev_end and ev_call1.  *launched
+// tells whether it ran; when it did not, nothing was enqueued.
+int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* stage,
+                            size_t a_bytes, int blocks, int threads, Readback* rb_host, cudaStream_t s,
+                            bool* launched)
+{
+    *launched = false;
+    SmallKernel kern = small_kernel(pb.n);
+    const size_t smem = small_call_smem_bytes(pb.n, pb.w, threads);
+    bool ok = false;
+    int st = small_call_ready(kern, pb, blocks, threads, ctx->device, ctx->sm_count, smem, &ok);
+    if (st != SPB_OK || !ok) return st;
+    if (!ctx->small_graphs) {
+        ctx->small_graphs = new SmallGraphCache();
+        ctx->release_small_graphs = release_cache;
+    }
+    SmallGraphCache* c = static_cast<SmallGraphCache*>(ctx->small_graphs);
+    SmallGraph* g = nullptr;
+    for (SmallGraph& x : c->e)
+        if (same_launch(x, pb, d_a, stage, a_bytes, rb_host, blocks, threads)) g = &x;
+    if (!g) {  // first sight of this launch: remember it, run it directly
+        SmallGraph* lru = &c->e[0];
+        for (SmallGraph& x : c->e)
+            if (!x.valid || x.stamp < lru->stamp) lru = &x;
+        if (lru->valid) drop(*lru);
+        lru->valid = true;
+        lru->pb = pb;
+        lru->a = d_a;
+        lru->stage = stage;
+        lru->a_bytes = a_bytes;
+        lru->rb_host = rb_host;
+        lru->blocks = blocks;
+        lru->threads = threads;
+        lru->uses = 1;
+        lru->stamp = ++c->clock;
+        return SPB_OK;
+    }
+    g->stamp = ++c->clock;
+    ++g->uses;
+    if (g->failed) return SPB_OK;
+    if (!g->exec) {
+        build(ctx, *g, kern, smem);
+        if (!g->exec) return SPB_OK;
+    }
+    SPB_CUDA_TRY(cudaGraphLaunch(g->exec, s));
     *launched = true;
     return SPB_OK;
 }

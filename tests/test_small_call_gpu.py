@@ -102,3 +102,29 @@ def test_fused_device_input_and_edge_values(spb):
     r = spb.perm_dense(sc, precision="dd")
     import math
     assert abs(r.permanent - math.factorial(12) * 0.75 ** 12) <= 1e-13 * r.permanent
+
+
+def test_fused_graph_replay_reads_each_matrix(spb, oracle):
+    """Repeated calls of one size replay the fused call as a CUDA graph, which
+    copies the matrix from the library's page-locked staging area: every call
+    must see its own matrix (host input) or its own device pointer."""
+    import ctypes
+    import torch
+    from superman_b200 import _lib
+    mats = [W.dense_uniform(20, 900 + k) for k in range(3)]
+    want = [spb.perm_dense(m, precision="dd", small_call=-1).permanent for m in mats]
+    for _ in range(3):  # first sight runs directly, then the graph replays
+        for m, w in zip(mats, want):
+            r = spb.perm_dense(m, precision="dd")
+            assert r.launches == 1
+            assert abs(r.permanent - w) <= 1e-15 * abs(w)
+    devs = [torch.from_numpy(m).cuda() for m in mats[:2]]
+    opt = _lib.default_options(precision=_lib.SPB_PREC_DD)
+    out = _lib.spb_result()
+    for _ in range(3):
+        for d, w in zip(devs, want[:2]):
+            _lib.check(_lib.lib().spb_perm_dense_f64_dev(ctypes.c_void_p(d.data_ptr()), 20, ctypes.byref(opt),
+                                                         ctypes.byref(out)))
+            assert abs(out.value - w) <= 1e-15 * abs(w)
+            assert out.device_s > 0.0 and out.kernel_s > 0.0 and out.kernel_s <= out.device_s
+    assert oracle.rel_err(want[0], oracle.exact_perm(mats[0])) <= 1e-13
