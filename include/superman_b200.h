@@ -84,6 +84,12 @@ typedef struct spb_options {
     int small_call;        /* >= 0: real matrices with 4 <= n <= 24 run as one
                               fused kernel (tables, walk, threshold and
                               refinement); < 0: as separate kernels        */
+    int skip_timing;       /* 1: the dense entry points skip their device
+                              timing (no elapsed-time queries; the replayed
+                              fused call records no events); kernel_s and
+                              device_s in spb_result are then 0.  About 6 us
+                              less per call, for callers that time calls
+                              themselves                                    */
 } spb_options;
 
 typedef struct spb_result {

@@ -53,6 +53,7 @@ class spb_options(ctypes.Structure):
         ("sparse_walk", ctypes.c_int),
         ("replay_listing", ctypes.c_int),
         ("small_call", ctypes.c_int),
+        ("skip_timing", ctypes.c_int),
     ]
 
 

@@ -186,10 +186,10 @@ size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * 
 // The fused small-matrix call (small_call.cu).
 constexpr int kSmallCallMaxN = 24;
 size_t small_call_smem_bytes(int n, int w, int threads);
-int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, Readback* rb_host, int dev,
-                      int sms, cudaStream_t s, bool* launched);
-int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* stage,
-                            size_t a_bytes, int blocks, int threads, Readback* rb_host, cudaStream_t s,
+int launch_small_call(const Problem& pb, const double* d_a, const double* a_stage, int blocks, int threads,
+                      Readback* rb_host, int dev, int sms, cudaStream_t s, bool* launched);
+int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* a_stage,
+                            int blocks, int threads, Readback* rb_host, bool timed, cudaStream_t s,
                             bool* launched);
 
 // The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
@@ -450,35 +450,42 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     // (small_call.cu), unless the device cannot hold its grid or its count
     // check fails, in which case the separate kernels below run.  The kernel
     // writes the finished readback straight into the pinned buffer when the
-    // device can address it (no copy after the kernel).  A launch asked for
-    // again is replayed as a CUDA graph (events, matrix copy from the
-    // pinned staging area, kernel): one graph launch instead of ~10 us of
-    // host calls during which the device waits.
+    // device can address it (no copy after the kernel), and takes a host
+    // matrix from the pinned staging area itself (no copy before it: a copy
+    // engine takes several microseconds to start for 4.6 KB).  A launch asked
+    // for again is replayed as a CUDA graph (events and kernel; the kernel
+    // alone with skip_timing).
     const bool fused_fits = small_candidate && pb.units <= (unsigned long long)blocks * threads &&
                             pb.units <= kRawCap && small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin;
     Readback* mapped = static_cast<Readback*>(ctx->pinned_dev);
-    bool fused = false, staged = false;
+    const double* a_stage = nullptr;  // device address of the staged host matrix
+    if (fused_fits && mapped && !a_on_device) {
+        std::memcpy(static_cast<char*>(ctx->pinned) + kStageOff, a, a_bytes);
+        a_stage = reinterpret_cast<const double*>(static_cast<char*>(ctx->pinned_dev) + kStageOff);
+    }
+    bool fused = false, graphed = false;
     if (fused_fits && mapped) {
-        double* stage = reinterpret_cast<double*>(static_cast<char*>(ctx->pinned) + kStageOff);
-        if (!a_on_device) std::memcpy(stage, a, a_bytes);
-        if ((st = launch_small_call_graph(ctx, pb, d_a, a_on_device ? nullptr : stage, a_bytes, blocks, threads,
-                                          mapped, stream, &fused)) != SPB_OK)
+        if ((st = launch_small_call_graph(ctx, pb, d_a, a_stage, blocks, threads, mapped, !opt.skip_timing, stream,
+                                          &fused)) != SPB_OK)
             return out->status = st;
-        staged = fused;
+        graphed = fused;
     }
-    if (!staged) {
+    if (!graphed) {
         SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call0, stream));
-        if (!a_on_device) SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, a_bytes, cudaMemcpyHostToDevice, stream));
-    }
-    if (fused_fits && !staged) {
-        SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
-        if ((st = launch_small_call(pb, d_a, blocks, threads, mapped, ctx->device, ctx->sm_count, stream,
-                                    &fused)) != SPB_OK)
-            return out->status = st;
-        if (fused) {
-            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
-            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
+        if (!a_on_device && !a_stage)
+            SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, a_bytes, cudaMemcpyHostToDevice, stream));
+        if (fused_fits) {
+            SPB_CUDA_TRY(cudaEventRecord(ctx->ev_begin, stream));
+            if ((st = launch_small_call(pb, d_a, a_stage, blocks, threads, mapped, ctx->device, ctx->sm_count,
+                                        stream, &fused)) != SPB_OK)
+                return out->status = st;
+            if (fused) {
+                SPB_CUDA_TRY(cudaEventRecord(ctx->ev_end, stream));
+                SPB_CUDA_TRY(cudaEventRecord(ctx->ev_call1, stream));
+            }
         }
+        // the fused call did not run: the separate kernels read the matrix at d_in
+        if (!fused && a_stage) SPB_CUDA_TRY(cudaMemcpyAsync(d_in, a, a_bytes, cudaMemcpyHostToDevice, stream));
     }
     if (fused) {
         if (!mapped) SPB_CUDA_TRY(cudaMemcpyAsync(hrb, pb.rb, sizeof(Readback), cudaMemcpyDeviceToHost, stream));
@@ -590,13 +597,15 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         for (int cc = 0; cc < comps; ++cc) res[cc] = dd_add(res0[cc], hrb->corr[cc]);
         out->refined_units = count;
         float mr = 0.f;
-        SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
+        if (!opt.skip_timing) SPB_CUDA_TRY(cudaEventElapsedTime(&mr, ctx->ev_ref0, ctx->ev_ref1));
         ms_refine = mr;
     }
     }  // separate kernels
     float ms = 0.f, ms_call = 0.f;
-    SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
-    SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));
+    if (!opt.skip_timing) {
+        SPB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev_begin, ctx->ev_end));
+        SPB_CUDA_TRY(cudaEventElapsedTime(&ms_call, ctx->ev_call0, ctx->ev_call1));
+    }
 
     // FP32 products: estimated relative error of the result from the sum of
     // squared terms s2 the walk accumulated.  A term carries k roundings of

@@ -112,8 +112,8 @@ static_assert(sizeof(Readback) % sizeof(unsigned long long) == 0, "readback copi
 __device__ __forceinline__ double* unit_value(const Problem& pb) { return reinterpret_cast<double*>(pb.raw_u); }
 
 template <int N>
-__global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* __restrict__ a_in,
-                                                                         Readback* rb_host)
+__global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem pb, const double* a_in,
+                                                                         const double* a_stage, Readback* rb_host)
 {
     constexpr int G = RealCfg<N>::G;
     cg::grid_group grid = cg::this_grid();
@@ -139,8 +139,12 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     float* s_hist = reinterpret_cast<float*>(smem + L.hist);
     unsigned* s_cnt = reinterpret_cast<unsigned*>(s_hist + kHistBins);
 
-    // ---- 0. tables (setup_kernel's operations) and the zeroed accumulators
-    for (int i = tid; i < N * N; i += bd) s_a[i] = a_in[i];
+    // ---- 0. the zeroed accumulators and the tables (setup_kernel's
+    // operations).  A host matrix arrives staged in page-locked memory
+    // (a_stage, mapped): the grid copies it to a_in first, one element per
+    // thread, and meets at a barrier, which also publishes the zeroed
+    // accumulators; a device matrix is read where it is.
+    const bool staged = a_stage != nullptr;  // the same in every CTA
     if (blockIdx.x == 0) {
         if (tid < 4) pb.ticket[tid] = 0u;
         if (mode != 0)
@@ -149,6 +153,14 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
                 pb.hist_cnt[i] = 0ull;
             }
         if (tid == 0) *pb.list_n = 0ull;
+    }
+    if (staged) {
+        double* a_dev = const_cast<double*>(a_in);
+        for (int i = blockIdx.x * bd + tid; i < N * N; i += gridDim.x * bd) a_dev[i] = a_stage[i];
+        grid.sync();
+        for (int i = tid; i < N * N; i += bd) s_a[i] = __ldcg(a_in + i);
+    } else {
+        for (int i = tid; i < N * N; i += bd) s_a[i] = a_in[i];
     }
     if (mode != 0)
         for (int i = tid; i < kHistBins; i += bd) { s_hist[i] = 0.0f; s_cnt[i] = 0u; }
@@ -213,7 +225,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         s_mt[idx] = s_a[r * N + (w + j)];
     }
     __syncthreads();
-    grid.sync();  // the zeroed accumulators are visible before anyone adds to them
+    if (!staged) grid.sync();  // the zeroed accumulators are visible before anyone adds to them
 
     // ---- 1. the walk: one unit per thread (units <= threads: thread t owns
     // unit t), evaluated as walk_real evaluates it.  The warp builds its 32
@@ -405,7 +417,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     }
 }
 
-using SmallKernel = void (*)(Problem, const double*, Readback*);
+using SmallKernel = void (*)(Problem, const double*, const double*, Readback*);
 
 SmallKernel small_kernel(int n)
 {
@@ -467,8 +479,8 @@ static int small_call_ready(SmallKernel kern, const Problem& pb, int blocks, int
 // SMs) if it can keep `blocks` CTAs of `threads` threads resident at once;
 // *launched tells whether it did.  rb_host (may be null): the device's
 // address of a page-locked copy of the readback, which the kernel fills last.
-int launch_small_call(const Problem& pb, const double* d_a, int blocks, int threads, Readback* rb_host, int dev,
-                      int sms, cudaStream_t s, bool* launched)
+int launch_small_call(const Problem& pb, const double* d_a, const double* a_stage, int blocks, int threads,
+                      Readback* rb_host, int dev, int sms, cudaStream_t s, bool* launched)
 {
     *launched = false;
     SmallKernel kern = small_kernel(pb.n);
@@ -478,22 +490,23 @@ int launch_small_call(const Problem& pb, const double* d_a, int blocks, int thre
     if (st != SPB_OK || !ok) return st;
     Problem p = pb;
     const double* a = d_a;
+    const double* as = a_stage;
     Readback* h = rb_host;
-    void* args[] = {&p, &a, &h};
+    void* args[] = {&p, &a, &as, &h};
     SPB_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(blocks), dim3(threads), args, smem, s));
     *launched = true;
     return SPB_OK;
 }
 
 // ---- the call as a CUDA graph --------------------------------------------
-// A call issues the events around it, the matrix copy and the cooperative
-// launch: about 10 us of host time, during which the device waits for the
-// launch.  Replayed as one graph (events, copy from the context's page-locked
-// staging, kernel) it costs one graph launch.  A graph is built for a launch
-// (the kernel's Problem, its matrix and readback addresses, the shape) the
-// second time that launch is asked for in a row of calls, and kept in a small
-// per-context cache; a matrix given on the device is part of the launch, so
-// a caller that passes a new device pointer each time keeps the direct path.
+// A call issues the events around it and the cooperative launch: several
+// microseconds of host time, during which the device waits for the launch.
+// Replayed as one graph (events and kernel) it costs one graph launch.  A
+// graph is built for a launch (the kernel's Problem, its matrix, staging and
+// readback addresses, the shape) the second time that launch is asked for,
+// and kept in a small per-context cache; a matrix given on the device is
+// part of the launch, so a caller that passes a new device pointer each time
+// keeps the direct path.
 namespace {
 
 struct SmallGraph {
@@ -502,11 +515,11 @@ struct SmallGraph {
     int uses = 0;
     unsigned long long stamp = 0;
     Problem pb{};
-    const double* a = nullptr;  // the matrix the kernel reads
-    const double* stage = nullptr;  // page-locked source of the matrix copy (host input) or null
-    size_t a_bytes = 0;
+    const double* a = nullptr;      // the matrix the kernel reads (or fills from the staging)
+    const double* stage = nullptr;  // device address of the page-locked staging (host input) or null
     Readback* rb_host = nullptr;
     int blocks = 0, threads = 0;
+    bool timed = true;  // the graph records the context's events around the kernel
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -531,15 +544,15 @@ void release_cache(void* p)
     delete c;
 }
 
-bool same_launch(const SmallGraph& g, const Problem& pb, const double* a, const double* stage, size_t a_bytes,
-                 Readback* rb_host, int blocks, int threads)
+bool same_launch(const SmallGraph& g, const Problem& pb, const double* a, const double* stage, Readback* rb_host,
+                 int blocks, int threads, bool timed)
 {
     return g.valid && std::memcmp(&g.pb, &pb, sizeof(Problem)) == 0 && g.a == a && g.stage == stage &&
-           g.a_bytes == a_bytes && g.rb_host == rb_host && g.blocks == blocks && g.threads == threads;
+           g.rb_host == rb_host && g.blocks == blocks && g.threads == threads && g.timed == timed;
 }
 
-// Captures events, copy and kernel on the context's own stream.  Any error
-// ends the capture and leaves the entry marked failed.
+// Captures events and kernel on the context's own stream.  Any error ends
+// the capture and leaves the entry marked failed.
 void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
 {
     cudaStream_t cs = ctx->stream;
@@ -550,16 +563,16 @@ void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
     }
     Problem p = g.pb;
     const double* a = g.a;
+    const double* as = g.stage;
     Readback* h = g.rb_host;
-    void* args[] = {&p, &a, &h};
-    cudaError_t e = cudaEventRecordWithFlags(ctx->ev_call0, cs, cudaEventRecordExternal);
-    if (e == cudaSuccess && g.stage)
-        e = cudaMemcpyAsync(const_cast<double*>(g.a), g.stage, g.a_bytes, cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_begin, cs, cudaEventRecordExternal);
+    void* args[] = {&p, &a, &as, &h};
+    cudaError_t e = cudaSuccess;
+    if (g.timed) e = cudaEventRecordWithFlags(ctx->ev_call0, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_begin, cs, cudaEventRecordExternal);
     if (e == cudaSuccess)
         e = cudaLaunchCooperativeKernel((const void*)kern, dim3(g.blocks), dim3(g.threads), args, smem, cs);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_end, cs, cudaEventRecordExternal);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev_call1, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_end, cs, cudaEventRecordExternal);
+    if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_call1, cs, cudaEventRecordExternal);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
     if (e == cudaSuccess) e = e2;
@@ -578,12 +591,13 @@ void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
 }  // namespace
 
 // The fused call through a cached graph, on stream s.  The kernel reads its
-// matrix at d_a; with host input, stage (page-locked, holding the matrix)
-// is copied there first, inside the graph.  The graph also records the
-// context's events ev_call0, ev_begin, ev_end and ev_call1.  *launched
-// tells whether it ran; when it did not, nothing was enqueued.
-int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* stage,
-                            size_t a_bytes, int blocks, int threads, Readback* rb_host, cudaStream_t s,
+// matrix at d_a; with host input, a_stage (the device address of the
+// page-locked staging that holds it) is copied there by the kernel first.
+// When timed, the graph also records the context's events ev_call0,
+// ev_begin, ev_end and ev_call1.  *launched tells whether it ran; when it did
+// not, nothing was enqueued.
+int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* a_stage,
+                            int blocks, int threads, Readback* rb_host, bool timed, cudaStream_t s,
                             bool* launched)
 {
     *launched = false;
@@ -599,7 +613,7 @@ int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double*
     SmallGraphCache* c = static_cast<SmallGraphCache*>(ctx->small_graphs);
     SmallGraph* g = nullptr;
     for (SmallGraph& x : c->e)
-        if (same_launch(x, pb, d_a, stage, a_bytes, rb_host, blocks, threads)) g = &x;
+        if (same_launch(x, pb, d_a, a_stage, rb_host, blocks, threads, timed)) g = &x;
     if (!g) {  // first sight of this launch: remember it, run it directly
         SmallGraph* lru = &c->e[0];
         for (SmallGraph& x : c->e)
@@ -608,8 +622,8 @@ int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double*
         lru->valid = true;
         lru->pb = pb;
         lru->a = d_a;
-        lru->stage = stage;
-        lru->a_bytes = a_bytes;
+        lru->stage = a_stage;
+        lru->timed = timed;
         lru->rb_host = rb_host;
         lru->blocks = blocks;
         lru->threads = threads;

@@ -128,3 +128,17 @@ def test_fused_graph_replay_reads_each_matrix(spb, oracle):
             assert abs(out.value - w) <= 1e-15 * abs(w)
             assert out.device_s > 0.0 and out.kernel_s > 0.0 and out.kernel_s <= out.device_s
     assert oracle.rel_err(want[0], oracle.exact_perm(mats[0])) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [16, 24, 28])
+def test_skip_timing_same_result(spb, n):
+    """skip_timing drops the device timing only: the same permanent (to the
+    last bits the order of the refinement's corrections can move), with
+    kernel_s reported as 0 (fused call at n <= 24, separate kernels above)."""
+    a = W.dense_uniform(n, 930 + n)
+    t = spb.perm_dense(a, precision="dd")
+    for _ in range(3):  # direct, then graph-replayed for the fused call
+        u = spb.perm_dense(a, precision="dd", skip_timing=1)
+        assert abs(u.permanent - t.permanent) <= 1e-15 * abs(t.permanent)
+        assert u.kernel_s == 0.0
+    assert t.kernel_s > 0.0
