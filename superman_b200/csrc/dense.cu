@@ -184,7 +184,7 @@ namespace dense {
 size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
 
 // The fused small-matrix call (small_call.cu).
-constexpr int kSmallCallMaxN = 24;
+constexpr int kSmallCallMaxN = 25;
 size_t small_call_smem_bytes(int n, int w, int threads);
 int launch_small_call(const Problem& pb, const double* d_a, const double* a_stage, int blocks, int threads,
                       Readback* rb_host, int dev, int sms, cudaStream_t s, bool* launched);
@@ -393,7 +393,7 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
         return out->status = SPB_ERR_INVALID;
     }
     // The fused small call (below) walks with fewer threads per CTA on every
-    // SM when the units would leave SMs idle at full CTAs (n = 19 .. 24:
+    // SM when the units would leave SMs idle at full CTAs (n = 19 .. 25:
     // 2^15 or 2^16 units fill 64 or 128 CTAs of 512 threads; 147 CTAs of 448
     // threads give each SM an eighth less to walk).
     const bool small_candidate = opt.small_call >= 0 && comps == 1 && pb.na == n && !pb.f32 && n >= 4 &&

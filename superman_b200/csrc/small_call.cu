@@ -47,7 +47,7 @@ namespace cg = cooperative_groups;
 namespace spb {
 namespace dense {
 
-constexpr int kSmallCallMaxN = 24;
+constexpr int kSmallCallMaxN = 25;
 constexpr int kSmallCallThreads = 512;
 
 namespace {
@@ -427,7 +427,7 @@ SmallKernel small_kernel(int n)
         SPB_SCASE(4) SPB_SCASE(5) SPB_SCASE(6) SPB_SCASE(7) SPB_SCASE(8) SPB_SCASE(9) SPB_SCASE(10)
         SPB_SCASE(11) SPB_SCASE(12) SPB_SCASE(13) SPB_SCASE(14) SPB_SCASE(15) SPB_SCASE(16)
         SPB_SCASE(17) SPB_SCASE(18) SPB_SCASE(19) SPB_SCASE(20) SPB_SCASE(21) SPB_SCASE(22)
-        SPB_SCASE(23) SPB_SCASE(24)
+        SPB_SCASE(23) SPB_SCASE(24) SPB_SCASE(25)
 #undef SPB_SCASE
     default: return nullptr;
     }
