@@ -81,7 +81,7 @@ typedef struct spb_options {
                               replaying the walk (its own unit bases) instead
                               of the first pass's list or the parallel scan;
                               same result, slower (for verification)        */
-    int small_call;        /* >= 0: real matrices with 4 <= n <= 25 run as one
+    int small_call;        /* >= 0: real matrices with 4 <= n <= 26 run as one
                               fused kernel (tables, walk, threshold and
                               refinement); < 0: as separate kernels        */
     int skip_timing;       /* 1: the dense entry points skip their device

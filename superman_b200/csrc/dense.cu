@@ -184,7 +184,7 @@ namespace dense {
 size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
 
 // The fused small-matrix call (small_call.cu).
-constexpr int kSmallCallMaxN = 25;
+constexpr int kSmallCallMaxN = 26;
 size_t small_call_smem_bytes(int n, int w, int threads);
 int launch_small_call(const Problem& pb, const double* d_a, const double* a_stage, int blocks, int threads,
                       Readback* rb_host, int dev, int sms, cudaStream_t s, bool* launched);
@@ -398,14 +398,16 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     // threads give each SM an eighth less to walk).
     const bool small_candidate = opt.small_call >= 0 && comps == 1 && pb.na == n && !pb.f32 && n >= 4 &&
                                  n <= kSmallCallMaxN && !opt.replay_listing;
-    if (small_candidate && opt.threads_per_block <= 0 && opt.blocks <= 0 &&
-        pb.units >= 256ull * (unsigned long long)ctx->sm_count) {
-        const unsigned long long per_sm = (pb.units + ctx->sm_count - 1) / ctx->sm_count;
-        const int t = (int)((per_sm + 31) / 32 * 32);
-        if (t <= threads) {
-            threads = t;
-            smem = smem_for(threads);
+    if (small_candidate && opt.threads_per_block <= 0 && opt.blocks <= 0) {
+        if (pb.units >= 256ull * (unsigned long long)ctx->sm_count) {
+            const unsigned long long per_sm = (pb.units + ctx->sm_count - 1) / ctx->sm_count;
+            const int t = (int)((per_sm + 31) / 32 * 32);
+            if (t <= threads) threads = t;
         }
+        // the fused kernel's tables, warp bases and histogram fit one CTA
+        // (n = 26: 480 threads; its 2^17 units then take two passes)
+        while (threads > 256 && small_call_smem_bytes(n, pb.w, threads) > ctx->smem_optin) threads -= 32;
+        smem = smem_for(threads);
     }
     int blocks = opt.blocks > 0 ? opt.blocks : ctx->sm_count;
     // never launch more threads than units
@@ -455,8 +457,8 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     // engine takes several microseconds to start for 4.6 KB).  A launch asked
     // for again is replayed as a CUDA graph (events and kernel; the kernel
     // alone with skip_timing).
-    const bool fused_fits = small_candidate && pb.units <= (unsigned long long)blocks * threads &&
-                            pb.units <= kRawCap && small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin;
+    const bool fused_fits = small_candidate && pb.units <= kRawCap &&
+                            small_call_smem_bytes(n, pb.w, threads) <= ctx->smem_optin;
     Readback* mapped = static_cast<Readback*>(ctx->pinned_dev);
     const double* a_stage = nullptr;  // device address of the staged host matrix
     if (fused_fits && mapped && !a_on_device) {

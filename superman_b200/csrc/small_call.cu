@@ -12,9 +12,10 @@
 //      and subset-sum table, the high columns and the per-row bound ranges,
 //      with the operations of setup_kernel, so the values are the same;
 //      CTA 0 also zeroes the call's global accumulators; grid barrier;
-//   1. evaluates one unit per thread (thread t owns unit t, the split
-//      walk_real makes when there are no more units than threads) with
-//      walk_real's evaluators, on unit bases its warp builds row-parallel
+//   1. evaluates the units in passes over the grid (thread t owns units t,
+//      t + T, ...; with no more units than the T threads of the grid, unit t
+//      alone, the split walk_real makes then) with walk_real's evaluators,
+//      on unit bases its warp builds row-parallel
 //      (double-double, so their hi words are walk_real's but for values
 //      within ~2^-104 of a rounding midpoint), binning each unit by its
 //      bound and recording the bin per unit; CTA totals go to pb.partials;
@@ -22,8 +23,8 @@
 //   2. every CTA sums the CTA totals in index order (the grid total, as
 //      grid_reduce forms it) and, with the refinement, picks the threshold
 //      from the histogram (one warp, pick_threshold);
-//   3. with the refinement, each thread lists its unit if it is at or above
-//      the threshold; grid barrier; the listed units are dealt out one per CTA
+//   3. with the refinement, each thread lists its units at or above the
+//      threshold; grid barrier; the listed units are dealt out one per CTA
 //      and re-evaluated by the whole CTA in double-double (base rebuilt from
 //      x0 and the high columns, as refine_real does), against the FP64 value
 //      the walk stored for the unit; the last CTA sums the corrections in
@@ -47,7 +48,7 @@ namespace cg = cooperative_groups;
 namespace spb {
 namespace dense {
 
-constexpr int kSmallCallMaxN = 25;
+constexpr int kSmallCallMaxN = 26;
 constexpr int kSmallCallThreads = 512;
 
 namespace {
@@ -227,87 +228,94 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __syncthreads();
     if (!staged) grid.sync();  // the zeroed accumulators are visible before anyone adds to them
 
-    // ---- 1. the walk: one unit per thread (units <= threads: thread t owns
-    // unit t), evaluated as walk_real evaluates it.  The warp builds its 32
-    // unit bases row-parallel: lane r adds the selected high columns of the
+    // ---- 1. the walk, one unit per thread and pass, evaluated as walk_real
+    // evaluates it.  In each pass the warp builds its 32 unit bases
+    // row-parallel: lane r adds the selected high columns of the
     // warp's first unit to x0_r in ascending order (double-double, as the
     // refinement rebuilds a base), then takes the 31 Gray steps to the
     // following units with walk_real's double-double step, storing each hi
     // word; each lane then reads its own unit's row values.  That is 16 adds
     // plus 31 steps per row and warp, where building each lane's base alone
     // costs every lane its own adds for all rows.
-    const unsigned long long u = (unsigned long long)blockIdx.x * bd + tid;
-    const unsigned long long ub = u - (unsigned long long)lane;  // the warp's first unit
-    double* s_base = smem + L.base + (size_t)wid * N * 33;       // [N][33]
-    if (ub < pb.units && lane < N) {
-        const int r = lane;
-        const unsigned long long g = gray_of(ub);
-        dd x = {s_x0h[r], s_x0l[r]};
-        for (int j = 0; j < ntop; ++j)
-            if ((g >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
-        s_base[r * 33] = x.hi;
-        for (int k = 1; k < 32 && ub + k < pb.units; ++k) {
-            const unsigned long long v = ub + k;
-            const int j = __ffsll((long long)v) - 1;
-            const double c = s_mt[j * N + r];
-            const dd sm = two_sum(x.hi, ((gray_of(v) >> j) & 1ull) ? c : -c);
-            x = fast_two_sum(sm.hi, add_rn(sm.lo, x.lo));
-            s_base[r * 33 + k] = x.hi;
-        }
-    }
-    __syncwarp();
+    // With more units than threads the grid takes them in passes: thread t
+    // owns units t, t + T, t + 2T, ... (T threads in the grid).
+    const unsigned long long T = (unsigned long long)gridDim.x * bd;
+    const unsigned long long t0 = (unsigned long long)blockIdx.x * bd + tid;
+    double* s_base = smem + L.base + (size_t)wid * N * 33;  // [N][33]
     dd tot = {0.0, 0.0};
-    HistCache hc;
-    if (u < pb.units) {
-        double xh[N];
+    for (unsigned long long u = t0;; u += T) {
+        const unsigned long long ub = u - (unsigned long long)lane;  // the warp's first unit
+        if (ub >= pb.units) break;  // the same in every lane of the warp
+        __syncwarp();               // the previous pass's bases are read
+        if (lane < N) {
+            const int r = lane;
+            const unsigned long long g = gray_of(ub);
+            dd x = {s_x0h[r], s_x0l[r]};
+            for (int j = 0; j < ntop; ++j)
+                if ((g >> j) & 1ull) x = dd_add_d(x, s_mt[j * N + r]);
+            s_base[r * 33] = x.hi;
+            for (int k = 1; k < 32 && ub + k < pb.units; ++k) {
+                const unsigned long long v = ub + k;
+                const int j = __ffsll((long long)v) - 1;
+                const double c = s_mt[j * N + r];
+                const dd sm = two_sum(x.hi, ((gray_of(v) >> j) & 1ull) ? c : -c);
+                x = fast_two_sum(sm.hi, add_rn(sm.lo, x.lo));
+                s_base[r * 33 + k] = x.hi;
+            }
+        }
+        __syncwarp();
+        int b = -1;  // this lane's histogram bin in this pass (-1: no unit)
+        double sq = 0.0;
+        if (u < pb.units) {
+            double xh[N];
 #pragma unroll
-        for (int r = 0; r < N; ++r) xh[r] = s_base[r * 33 + lane];
-        if (mode == 0) {
-            const double us = unit_sum_real<N, G>(xh, s_dh, nq);
-            tot = dd_add_d(tot, (u & 1ull) ? -us : us);
-        } else {
-            double ubd = 1.0;
+            for (int r = 0; r < N; ++r) xh[r] = s_base[r * 33 + lane];
+            if (mode == 0) {
+                const double us = unit_sum_real<N, G>(xh, s_dh, nq);
+                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+            } else {
+                double ubd = 1.0;
 #pragma unroll
-            for (int r = 0; r < N; ++r)
-                ubd = mul_rn(ubd, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
-            const int b = hist_bin(ubd);
-            pb.raw_b[u] = (unsigned short)b;
-            double sq;
-            const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
-            tot = dd_add_d(tot, (u & 1ull) ? -us : us);
-            hc.add(b, sq, s_hist, s_cnt);
-            unit_value(pb)[u] = us;  // what the refinement corrects
+                for (int r = 0; r < N; ++r)
+                    ubd = mul_rn(ubd, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
+                b = hist_bin(ubd);
+                pb.raw_b[u] = (unsigned short)b;
+                const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
+                tot = dd_add_d(tot, (u & 1ull) ? -us : us);
+                unit_value(pb)[u] = us;  // what the refinement corrects
+            }
+        }
+        if (mode != 0) {
+            // Neighbouring units share bins, so the lanes of a warp with the
+            // same bin are summed by shuffles first and one shared atomic per
+            // bin and warp is issued.
+            const unsigned full = 0xffffffffu;
+            float v = 0.0f;
+            if (b >= 0) {
+                const double h = hist_half_unscale(b);
+                v = __double2float_rn((sq * h) * h);
+            }
+            unsigned pending = __ballot_sync(full, b >= 0);
+            while (pending) {
+                const int leader = __ffs(pending) - 1;
+                const int lb = __shfl_sync(full, b, leader);
+                const bool mine = b == lb;
+                float x = mine ? v : 0.0f;
+                unsigned c = mine ? 1u : 0u;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    x += __shfl_xor_sync(full, x, off);
+                    c += __shfl_xor_sync(full, c, off);
+                }
+                if (lane == leader) {
+                    atomicAdd(&s_hist[lb], x);
+                    atomicAdd(&s_cnt[lb], c);
+                }
+                pending &= ~__ballot_sync(full, mine);
+            }
         }
     }
     if (mode != 0) {
-        // Each thread walked at most one unit, and neighbouring units share
-        // bins, so the lanes of a warp with the same bin are summed by
-        // shuffles first and one shared atomic per bin and warp is issued.
-        const unsigned full = 0xffffffffu;
-        const int b = hc.cnt ? hc.bin : -1;
-        float v = 0.0f;
-        if (hc.cnt) {
-            const double h = hist_half_unscale(hc.bin);
-            v = __double2float_rn((hc.s2 * h) * h);
-        }
-        unsigned pending = __ballot_sync(full, b >= 0);
-        while (pending) {
-            const int leader = __ffs(pending) - 1;
-            const int lb = __shfl_sync(full, b, leader);
-            const bool mine = b == lb;
-            float x = mine ? v : 0.0f;
-            unsigned c = mine ? hc.cnt : 0u;
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                x += __shfl_xor_sync(full, x, off);
-                c += __shfl_xor_sync(full, c, off);
-            }
-            if (lane == leader) {
-                atomicAdd(&s_hist[lb], x);
-                atomicAdd(&s_cnt[lb], c);
-            }
-            pending &= ~__ballot_sync(full, mine);
-        }
         __syncthreads();
         flush_hist(s_hist, s_cnt, pb);
     }
@@ -346,15 +354,16 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     if (mode == 0 || s_thr >= kHistBins) return;  // nothing to refine (uniform over the grid)
 
     // ---- 3. refinement of the units at or above the threshold.  Each thread
-    // lists its unit if it qualifies; after a grid barrier the listed units
+    // lists its units that qualify; after a grid barrier the listed units
     // are dealt out one per CTA in list order, so a cluster of dominant units
     // (they gather near the empty and the full subsets) spreads over the grid,
     // and each is refined by a whole CTA.
     const int thr = s_thr;
-    if (u < pb.units && (int)pb.raw_b[u] >= thr) {
-        const unsigned long long k = atomicAdd(pb.list_n, 1ull);
-        if (k < pb.list_cap) pb.list_u[k] = u;
-    }
+    for (unsigned long long u = t0; u < pb.units; u += T)
+        if ((int)pb.raw_b[u] >= thr) {
+            const unsigned long long k = atomicAdd(pb.list_n, 1ull);
+            if (k < pb.list_cap) pb.list_u[k] = u;
+        }
     grid.sync();
     const unsigned long long listed = __ldcg(pb.list_n);
     const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
@@ -427,7 +436,7 @@ SmallKernel small_kernel(int n)
         SPB_SCASE(4) SPB_SCASE(5) SPB_SCASE(6) SPB_SCASE(7) SPB_SCASE(8) SPB_SCASE(9) SPB_SCASE(10)
         SPB_SCASE(11) SPB_SCASE(12) SPB_SCASE(13) SPB_SCASE(14) SPB_SCASE(15) SPB_SCASE(16)
         SPB_SCASE(17) SPB_SCASE(18) SPB_SCASE(19) SPB_SCASE(20) SPB_SCASE(21) SPB_SCASE(22)
-        SPB_SCASE(23) SPB_SCASE(24) SPB_SCASE(25)
+        SPB_SCASE(23) SPB_SCASE(24) SPB_SCASE(25) SPB_SCASE(26)
 #undef SPB_SCASE
     default: return nullptr;
     }

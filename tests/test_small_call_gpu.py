@@ -1,4 +1,4 @@
-"""The fused small-matrix call (one cooperative kernel for real 4 <= n <= 25:
+"""The fused small-matrix call (one cooperative kernel for real 4 <= n <= 26:
 tables, walk, threshold and double-double refinement) against the same call
 made of separate kernels, and against the exact value."""
 import numpy as np
@@ -47,7 +47,7 @@ def test_fused_launch_shapes(spb, oracle, n, threads):
     assert oracle.rel_err(r.permanent + r.permanent_lo, oracle.exact_perm(a)) <= 1e-13
 
 
-@pytest.mark.parametrize("n", [6, 12, 18, 21, 24, 25])
+@pytest.mark.parametrize("n", [6, 12, 18, 21, 24, 25, 26])
 def test_fused_dd_matches_separate_and_exact(spb, oracle, n):
     a = W.dense_uniform(n, 710 + n)
     f = spb.perm_dense(a, precision="dd")
@@ -130,11 +130,11 @@ def test_fused_graph_replay_reads_each_matrix(spb, oracle):
     assert oracle.rel_err(want[0], oracle.exact_perm(mats[0])) <= 1e-13
 
 
-@pytest.mark.parametrize("n", [16, 24, 28])
+@pytest.mark.parametrize("n", [16, 24, 26, 28])
 def test_skip_timing_same_result(spb, n):
     """skip_timing drops the device timing only: the same permanent (to the
     last bits the order of the refinement's corrections can move), with
-    kernel_s reported as 0 (fused call at n <= 25, separate kernels above)."""
+    kernel_s reported as 0 (fused call at n <= 26, separate kernels above)."""
     a = W.dense_uniform(n, 930 + n)
     t = spb.perm_dense(a, precision="dd")
     for _ in range(3):  # direct, then graph-replayed for the fused call
