@@ -29,21 +29,11 @@ def test_fused_equals_separate_fp64(spb, n):
 
 @pytest.mark.parametrize("n,threads", [(12, 96), (20, 160), (20, 384), (22, 448), (24, 448), (24, 384)])
 def test_fused_launch_shapes(spb, oracle, n, threads):
-    """CTAs of fewer threads: the fused call runs whenever every unit has a
-    thread of the one-CTA-per-SM grid, and is exact to the bar either way."""
-    import torch
+    """CTAs of fewer threads: the grid takes the units in passes (thread t
+    owns units t, t + T, ...), one launch, exact to the bar."""
     a = W.dense_uniform(n, 720 + n)
     r = spb.perm_dense(a, precision="dd", threads_per_block=threads)
-    w = 8  # the library's default unit width: a 64 KB table, >= 2^16 units when n allows
-    while w > 2 and (1 << w) * n * 8 > 64 * 1024:
-        w -= 1
-    while w > 2 and n - 1 - w < 16 and w > n - 17:
-        w -= 1
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    if 2 ** (n - 1 - w) <= sms * threads:
-        assert r.launches == 1
-    else:
-        assert r.launches >= 2
+    assert r.launches == 1
     assert oracle.rel_err(r.permanent + r.permanent_lo, oracle.exact_perm(a)) <= 1e-13
 
 
