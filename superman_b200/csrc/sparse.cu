@@ -87,10 +87,13 @@ void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, bool
     // memory.
     int wmax = std::min(10, n - 1 - min_ntop);
     while (wmax > 2 && ((size_t)1 << wmax) * (size_t)n * sizeof(double) > (size_t)64 * 1024) --wmax;
+    std::vector<int> high(n), key(n), start(n + 2);
+    std::vector<char> used(n);
+    std::vector<int> low;
     for (int last = 0; last < n; ++last) {
-        std::vector<char> used(n, 0);
+        std::fill(used.begin(), used.end(), 0);
         used[last] = 1;
-        std::vector<int> low;
+        low.clear();
         unsigned long long U = 0;
         for (int w = 1; w <= wmax; ++w) {
             int bj = -1, bu = 1 << 30, bc = 1 << 30;
@@ -105,20 +108,27 @@ void choose(const std::vector<unsigned long long>& cm, int n, int min_ntop, bool
             U |= cm[bj];
             const int na = popc(U);
             if (w < 2 || na < 1 || na >= n || na > kMaxActive) continue;
-            std::vector<int> high;
+            // the unused columns by ascending count of nonzeros outside U,
+            // ties by index (a stable counting sort: keys are at most n)
+            std::fill(start.begin(), start.end(), 0);
             for (int c = 0; c < n; ++c)
-                if (!used[c]) high.push_back(c);
-            std::stable_sort(high.begin(), high.end(),
-                             [&](int x, int y) { return popc(cm[x] & ~U) < popc(cm[y] & ~U); });
+                if (!used[c]) {
+                    key[c] = popc(cm[c] & ~U);
+                    ++start[key[c] + 1];
+                }
+            for (int k = 0; k <= n; ++k) start[k + 1] += start[k];
+            const int nh = start[n + 1];
+            for (int c = 0; c < n; ++c)
+                if (!used[c]) high[start[key[c]]++] = c;
             double flip = 0.0;
-            for (size_t j = 0; j < high.size(); ++j) flip += std::ldexp((double)popc(cm[high[j]] & ~U), -(int)j - 1);
+            for (int j = 0; j < nh; ++j) flip += std::ldexp((double)key[high[j]], -j - 1);
             const double cost = walk_cost(n, w, na, flip, dd);
             if (cost < best->cost) {
                 best->cost = cost;
                 best->na = na;
                 best->w = w;
                 best->cols = low;
-                best->cols.insert(best->cols.end(), high.begin(), high.end());
+                best->cols.insert(best->cols.end(), high.begin(), high.begin() + nh);
                 best->cols.push_back(last);
                 best->rows.clear();
                 for (int r = 0; r < n; ++r)
