@@ -510,7 +510,8 @@ int launch_small_call(const Problem& pb, const double* d_a, const double* a_stag
 // ---- the call as a CUDA graph --------------------------------------------
 // A call issues the events around it and the cooperative launch: several
 // microseconds of host time, during which the device waits for the launch.
-// Replayed as one graph (events and kernel) it costs one graph launch.  A
+// Replayed as one graph (the kernel between two events) it costs one graph
+// launch.  A
 // graph is built for a launch (the kernel's Problem, its matrix, staging and
 // readback addresses, the shape) the second time that launch is asked for,
 // and kept in a small per-context cache; a matrix given on the device is
@@ -576,12 +577,10 @@ void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
     Readback* h = g.rb_host;
     void* args[] = {&p, &a, &as, &h};
     cudaError_t e = cudaSuccess;
-    if (g.timed) e = cudaEventRecordWithFlags(ctx->ev_call0, cs, cudaEventRecordExternal);
-    if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_begin, cs, cudaEventRecordExternal);
+    if (g.timed) e = cudaEventRecordWithFlags(ctx->ev_begin, cs, cudaEventRecordExternal);
     if (e == cudaSuccess)
         e = cudaLaunchCooperativeKernel((const void*)kern, dim3(g.blocks), dim3(g.threads), args, smem, cs);
     if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_end, cs, cudaEventRecordExternal);
-    if (e == cudaSuccess && g.timed) e = cudaEventRecordWithFlags(ctx->ev_call1, cs, cudaEventRecordExternal);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
     if (e == cudaSuccess) e = e2;
@@ -602,9 +601,10 @@ void build(DeviceContext* ctx, SmallGraph& g, SmallKernel kern, size_t smem)
 // The fused call through a cached graph, on stream s.  The kernel reads its
 // matrix at d_a; with host input, a_stage (the device address of the
 // page-locked staging that holds it) is copied there by the kernel first.
-// When timed, the graph also records the context's events ev_call0,
-// ev_begin, ev_end and ev_call1.  *launched tells whether it ran; when it did
-// not, nothing was enqueued.
+// When timed, the graph also records the context's events ev_begin and
+// ev_end around the kernel, which is then the whole call on the device (the
+// matrix copy is its first step).  *launched tells whether it ran; when it
+// did not, nothing was enqueued.
 int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double* d_a, const double* a_stage,
                             int blocks, int threads, Readback* rb_host, bool timed, cudaStream_t s,
                             bool* launched)
