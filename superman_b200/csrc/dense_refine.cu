@@ -223,8 +223,17 @@ __global__ void __launch_bounds__(32) dd_threshold(Problem pb)
 {
     const int lane = threadIdx.x;
     Readback* rb = pb.rb;
+    // the histogram staged in shared memory with coalesced loads (read in
+    // place, each lane's 16 consecutive bins cost one L2 request per bin)
+    __shared__ double s_h2[kHistPadded];
+    __shared__ unsigned long long s_hc[kHistPadded];
+    for (int b = lane; b < kHistBins; b += 32) {
+        s_h2[hist_pad_index(b)] = __ldcg(pb.hist_s2 + b);
+        s_hc[hist_pad_index(b)] = __ldcg(pb.hist_cnt + b);
+    }
+    __syncwarp();
     const double mag = pb.comps == 1 ? fabs(rb->res[0].hi) : hypot(rb->res[0].hi, rb->res[1].hi);
-    const ThresholdPick t = pick_threshold(pb, mag);
+    const ThresholdPick t = pick_threshold_shared(pb, mag, s_h2, s_hc);
     if (lane == 0) {
         rb->thr = t.thr;
         rb->count = t.count;

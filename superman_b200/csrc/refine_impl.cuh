@@ -50,15 +50,26 @@ __device__ __forceinline__ double group_sum_real_rt(const double* xh, const doub
 // estimate is reported instead.  Called by all 32 lanes of one warp; lane l
 // owns bins [16l, 16l + 16), and the cumulative sums over bins are lane-local
 // sums joined by warp scans (a fixed order, so the result is deterministic).
-// The histogram is read through L2 (it was written by atomics of other CTAs).
-// Every lane returns the result.
+// The histogram is read from a copy in shared memory laid out by
+// hist_pad_index (staged with coalesced loads through L2: it was written by
+// atomics of other CTAs).  Every lane returns the result.
 struct ThresholdPick {
     int thr;                   // refinement bin (kHistBins: none)
     unsigned long long count;  // units at or above it
     double err;                // expected relative error of the units below it
 };
 
-__device__ __forceinline__ ThresholdPick pick_threshold(const Problem& pb, double mag)
+// Shared-memory position of bin b in a staged copy of the histogram: each
+// lane's 16 consecutive bins are one row of 17, so the lanes' reads of their
+// i-th bins fall in different banks (two lanes per bank pair).
+__host__ __device__ constexpr int hist_pad_index(int b)
+{
+    return (b / (kHistBins / 32)) * (kHistBins / 32 + 1) + b % (kHistBins / 32);
+}
+constexpr int kHistPadded = 32 * (kHistBins / 32 + 1);
+
+__device__ __forceinline__ ThresholdPick pick_threshold_shared(const Problem& pb, double mag, const double* s_s2,
+                                                               const unsigned long long* s_cnt)
 {
     constexpr int kPer = kHistBins / 32;
     const int lane = threadIdx.x & 31;
@@ -73,8 +84,9 @@ __device__ __forceinline__ ThresholdPick pick_threshold(const Problem& pb, doubl
     unsigned long long cl = 0;
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        v[i] = mul_rn(__ldcg(pb.hist_s2 + lane * kPer + i), var_per_s2);
-        cn[i] = __ldcg(pb.hist_cnt + lane * kPer + i);
+        const int b = lane * kPer + i;
+        v[i] = mul_rn(s_s2[hist_pad_index(b)], var_per_s2);
+        cn[i] = s_cnt[hist_pad_index(b)];
         loc = add_rn(loc, v[i]);
         cl += cn[i];
     }

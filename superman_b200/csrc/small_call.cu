@@ -22,7 +22,8 @@
 //      grid barrier;
 //   2. every CTA sums the CTA totals in index order (the grid total, as
 //      grid_reduce forms it) and, with the refinement, picks the threshold
-//      from the histogram (one warp, pick_threshold);
+//      from the histogram (staged in shared memory; one warp,
+//      pick_threshold_shared);
 //   3. with the refinement, each thread lists its units at or above the
 //      threshold; grid barrier; the listed units are dealt out one per CTA
 //      and re-evaluated by the whole CTA in double-double (base rebuilt from
@@ -69,8 +70,12 @@ struct SmallLayout {
         dh = even(x0l + n);
         dl = even(dh + terms * n);
         mt = even(dl + terms * n);
-        base = even(mt + ntop * n);              // [warps][n][33] the walk's unit bases (hi words)
-        bnd = even(base + warps * (size_t)n * 33);
+        // [warps][n][33] the walk's unit bases (hi words); after the walk, the
+        // staged histogram (2 x kHistPadded doubles)
+        base = even(mt + ntop * n);
+        const size_t nb = warps * (size_t)n * 33 > 2 * (size_t)kHistPadded ? warps * (size_t)n * 33
+                                                                           : 2 * (size_t)kHistPadded;
+        bnd = even(base + nb);
         xw = even(bnd + 2 * (size_t)n);          // [2n] the refined unit's base, hi then lo
         hist = even(xw + 2 * (size_t)n);          // float[kHistBins] + unsigned[kHistBins]
         total = hist + (kHistSmemBytes + sizeof(double) - 1) / sizeof(double);
@@ -324,14 +329,26 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     if (tid == 0) pb.partials[blockIdx.x] = cta;
     grid.sync();
 
-    // ---- 2. grid total (index order, every CTA alike) and the threshold
+    // ---- 2. grid total (index order, every CTA alike) and the threshold.
+    // The whole CTA first copies the histogram into shared memory (the unit
+    // bases' space, free now) with coalesced loads: read directly, each
+    // lane's 16 consecutive bins cost one L2 request per bin.
+    double* s_h2 = smem + L.base;
+    unsigned long long* s_hc = reinterpret_cast<unsigned long long*>(s_h2 + kHistPadded);
+    if (mode != 0) {
+        for (int b = tid; b < kHistBins; b += bd) {
+            s_h2[hist_pad_index(b)] = __ldcg(pb.hist_s2 + b);
+            s_hc[hist_pad_index(b)] = __ldcg(pb.hist_cnt + b);
+        }
+        __syncthreads();
+    }
     if (wid == 0) {
         dd v = lane_sum_dd(pb.partials, (int)gridDim.x, lane);
         v = warp_sum_dd(v);
         if (lane == 0) s_total = v;
         if (mode != 0) {
             const double mag = fabs(v.hi);
-            const ThresholdPick pk = pick_threshold(pb, mag);
+            const ThresholdPick pk = pick_threshold_shared(pb, mag, s_h2, s_hc);
             if (lane == 0) {
                 s_thr = pk.thr;
                 s_count = pk.count;
