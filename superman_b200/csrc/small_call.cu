@@ -186,12 +186,17 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     __syncthreads();
     for (int i = tid; i < N * N; i += bd) s_a[i] = ldexp(s_a[i], -s_exp[i / N]);
     __syncthreads();
-    if (blockIdx.x == 0 && tid == bd - 1) {  // not a row thread (bd >= 32 > N): the x0 sums start at once
-        int es = 0;
-        for (int r = 0; r < N; ++r) es += s_exp[r];
-        *pb.exp_sum = es;
-    }
-    for (int r = tid; r < N; r += bd) {
+    // The NW start vector x0 (one row per lane of the CTA's last warp, n
+    // dependent adds each) and the subset-sum table (every other thread)
+    // are built side by side.  Each table entry DE[d][r] is the sum of
+    // row r's entries over the bits of d, added in ascending bit order: the
+    // operations and order of a level-by-level build DE[d] = DE[d - 2^k] +
+    // a_rk (k the top bit of d), without its barriers.  Layout
+    // [d/G][r][d%G].
+    auto pos = [&](int d, int r) { return ((d / G) * N + r) * G + (d % G); };
+    const int xw0 = bd >= 64 ? bd - 32 : 0;  // the x0 warp
+    if (tid >= xw0 && tid - xw0 < N) {
+        const int r = tid - xw0;
         dd s = {0.0, 0.0};
         for (int j = 0; j < N; ++j) s = dd_add_d(s, s_a[r * N + j]);
         dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
@@ -199,23 +204,21 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         s_x0h[r] = x.hi;
         s_x0l[r] = x.lo;
     }
-    // subset sums level by level: DE[d] = DE[d - 2^k] + a_k, grouped [d/G][r][d%G]
-    auto pos = [&](int d, int r) { return ((d / G) * N + r) * G + (d % G); };
-    for (int r = tid; r < N; r += bd) {
-        s_dh[pos(0, r)] = 0.0;
-        s_dl[pos(0, r)] = 0.0;
+    if (blockIdx.x == 0 && tid == bd - 1) {  // lane 31 of the x0 warp: not a row thread (N < 32)
+        int es = 0;
+        for (int r = 0; r < N; ++r) es += s_exp[r];
+        *pb.exp_sum = es;
     }
-    for (int k = 0; k < w; ++k) {
-        __syncthreads();
-        const int half = 1 << k;
-        for (int idx = tid; idx < half * N; idx += bd) {
-            const int d = half + idx / N, r = idx % N;
-            const int from = pos(d - half, r);
-            const dd s = dd_add_d(dd{s_dh[from], s_dl[from]}, s_a[r * N + k]);
+    const int nde = bd >= 64 ? bd - 32 : bd;  // threads building the table
+    if (tid < nde)
+        for (int idx = tid; idx < terms * N; idx += nde) {
+            const int d = idx / N, r = idx % N;
+            dd s = {0.0, 0.0};
+            for (int j = 0; j < w; ++j)
+                if ((d >> j) & 1) s = dd_add_d(s, s_a[r * N + j]);
             s_dh[pos(d, r)] = s.hi;
             s_dl[pos(d, r)] = s.lo;
         }
-    }
     if (mode != 0)
         for (int r = tid; r < N; r += bd) {
             double lo = 0.0, hi = 0.0;
