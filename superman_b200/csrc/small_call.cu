@@ -187,16 +187,16 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     for (int i = tid; i < N * N; i += bd) s_a[i] = ldexp(s_a[i], -s_exp[i / N]);
     __syncthreads();
     // The NW start vector x0 (one row per lane of the CTA's last warp, n
-    // dependent adds each) and the subset-sum table (every other thread)
-    // are built side by side.  Each table entry DE[d][r] is the sum of
-    // row r's entries over the bits of d, added in ascending bit order: the
-    // operations and order of a level-by-level build DE[d] = DE[d - 2^k] +
-    // a_rk (k the top bit of d), without its barriers.  Layout
-    // [d/G][r][d%G].
+    // dependent adds each) and the subset-sum table (the other warps, a row
+    // each at a time) are built side by side.  A row's table is built level
+    // by level, DE[d][r] = DE[d - 2^k][r] + a_rk for d in [2^k, 2^(k+1)),
+    // its lanes taking a level's entries and meeting at a warp barrier; the
+    // values are setup_kernel's.  Layout [d/G][r][d%G].
     auto pos = [&](int d, int r) { return ((d / G) * N + r) * G + (d % G); };
-    const int xw0 = bd >= 64 ? bd - 32 : 0;  // the x0 warp
-    if (tid >= xw0 && tid - xw0 < N) {
-        const int r = tid - xw0;
+    const int nw = bd >> 5;
+    const int xwarp = nw > 1 ? nw - 1 : 0;  // the x0 warp
+    if (wid == xwarp && lane < N) {
+        const int r = lane;
         dd s = {0.0, 0.0};
         for (int j = 0; j < N; ++j) s = dd_add_d(s, s_a[r * N + j]);
         dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
@@ -209,15 +209,36 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         for (int r = 0; r < N; ++r) es += s_exp[r];
         *pb.exp_sum = es;
     }
-    const int nde = bd >= 64 ? bd - 32 : bd;  // threads building the table
-    if (tid < nde)
-        for (int idx = tid; idx < terms * N; idx += nde) {
-            const int d = idx / N, r = idx % N;
-            dd s = {0.0, 0.0};
-            for (int j = 0; j < w; ++j)
-                if ((d >> j) & 1) s = dd_add_d(s, s_a[r * N + j]);
-            s_dh[pos(d, r)] = s.hi;
-            s_dl[pos(d, r)] = s.lo;
+    const int tw = nw > 1 ? nw - 1 : 1;  // warps building the table
+    if (wid < tw)
+        for (int r0 = wid; r0 < N; r0 += 2 * tw) {
+            // two rows side by side (independent chains); r1 may be past n
+            const int r1 = r0 + tw;
+            const bool two = r1 < N;
+            if (lane == 0) {
+                s_dh[pos(0, r0)] = 0.0;
+                s_dl[pos(0, r0)] = 0.0;
+                if (two) {
+                    s_dh[pos(0, r1)] = 0.0;
+                    s_dl[pos(0, r1)] = 0.0;
+                }
+            }
+            for (int k = 0; k < w; ++k) {
+                __syncwarp();
+                const int half = 1 << k;
+                const double a0 = s_a[r0 * N + k], a1 = two ? s_a[r1 * N + k] : 0.0;
+                for (int e = lane; e < half; e += 32) {
+                    const dd v0 = dd_add_d(dd{s_dh[pos(e, r0)], s_dl[pos(e, r0)]}, a0);
+                    if (two) {
+                        const dd v1 = dd_add_d(dd{s_dh[pos(e, r1)], s_dl[pos(e, r1)]}, a1);
+                        s_dh[pos(half + e, r1)] = v1.hi;
+                        s_dl[pos(half + e, r1)] = v1.lo;
+                    }
+                    s_dh[pos(half + e, r0)] = v0.hi;
+                    s_dl[pos(half + e, r0)] = v0.lo;
+                }
+            }
+            __syncwarp();
         }
     if (mode != 0)
         for (int r = tid; r < N; r += bd) {
