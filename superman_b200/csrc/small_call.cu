@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     const unsigned long long t0 = (unsigned long long)blockIdx.x * bd + tid;
     double* s_base = smem + L.base + (size_t)wid * N * 33;  // [N][33]
     dd tot = {0.0, 0.0};
+    int bin0 = -1, bin1 = -1;  // this thread's bins in the first two passes (listing reads the rest back)
     for (unsigned long long u = t0;; u += T) {
         const unsigned long long ub = u - (unsigned long long)lane;  // the warp's first unit
         if (ub >= pb.units) break;  // the same in every lane of the warp
@@ -309,6 +310,8 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
                     ubd = mul_rn(ubd, fmax(fabs(add_rn(xh[r], s_bnd[r])), fabs(add_rn(xh[r], s_bnd[N + r]))));
                 b = hist_bin(ubd);
                 pb.raw_b[u] = (unsigned short)b;
+                if (u == t0) bin0 = b;
+                else if (u == t0 + T) bin1 = b;
                 const double us = unit_sum_real<N, G, true>(xh, s_dh, nq, &sq);
                 tot = dd_add_d(tot, (u & 1ull) ? -us : us);
                 unit_value(pb)[u] = us;  // what the refinement corrects
@@ -359,6 +362,8 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     // lane's 16 consecutive bins cost one L2 request per bin.
     double* s_h2 = smem + L.base;
     unsigned long long* s_hc = reinterpret_cast<unsigned long long*>(s_h2 + kHistPadded);
+    dd v = {0.0, 0.0};
+    if (wid == 0) v = lane_sum_dd(pb.partials, (int)gridDim.x, lane);  // its loads overlap the staging
     if (mode != 0) {
         for (int b = tid; b < kHistBins; b += bd) {
             s_h2[hist_pad_index(b)] = __ldcg(pb.hist_s2 + b);
@@ -367,7 +372,6 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         __syncthreads();
     }
     if (wid == 0) {
-        dd v = lane_sum_dd(pb.partials, (int)gridDim.x, lane);
         v = warp_sum_dd(v);
         if (lane == 0) s_total = v;
         if (mode != 0) {
@@ -400,11 +404,13 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     // (they gather near the empty and the full subsets) spreads over the grid,
     // and each is refined by a whole CTA.
     const int thr = s_thr;
-    for (unsigned long long u = t0; u < pb.units; u += T)
-        if ((int)pb.raw_b[u] >= thr) {
+    for (unsigned long long u = t0; u < pb.units; u += T) {
+        const int b = u == t0 ? bin0 : (u == t0 + T ? bin1 : (int)pb.raw_b[u]);
+        if (b >= thr) {
             const unsigned long long k = atomicAdd(pb.list_n, 1ull);
             if (k < pb.list_cap) pb.list_u[k] = u;
         }
+    }
     grid.sync();
     const unsigned long long listed = __ldcg(pb.list_n);
     const unsigned long long nl = listed < pb.list_cap ? listed : 0ull;  // overflow: the host falls back
@@ -418,6 +424,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
     dd corr = {0.0, 0.0};
     for (unsigned long long k = blockIdx.x; k < nl; k += gridDim.x) {
         const unsigned long long u = __ldcg(pb.list_u + k);
+        const double walked = __ldcg(unit_value(pb) + u);  // in flight during the rebuild
         const unsigned long long g = gray_of(u);
         // unit base rebuilt from scratch in double-double (x0 plus the
         // selected high columns in index order), as refine_real does
@@ -442,7 +449,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         acc = block_sum_dd(acc, s_warp);
         if (tid == 0) {
             // against the value the walk added for this unit
-            dd c = dd_add_d(acc, -__ldcg(unit_value(pb) + u));
+            dd c = dd_add_d(acc, -walked);
             if (u & 1ull) c = dd_neg(c);
             corr = dd_add(corr, c);
         }
