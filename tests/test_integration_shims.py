@@ -1,10 +1,10 @@
-"""The reference-side bindings shown in INTEGRATION.md compile against the
-reference's own headers (CPU only; needs the reference sources, so it is
-skipped where they are absent).
+"""The reference-side bindings shown in the repository's integration guide
+compile against the reference's own headers (CPU only; needs the reference
+sources, so it is skipped where they are absent).
 
 The dense driver shim (section 1), the complex shim (section 2) and the
-sparse driver shim (section 2b) are cut out of INTEGRATION.md as a
-maintainer would paste them, put in one translation unit after the
+sparse driver shim (section 2b) are cut out of the guide as a maintainer
+would paste them, put in one translation unit after the
 reference's headers (CommonFiles/Permanent.h, Structures/SparseMatrix.h,
 CommonFiles/Helpers.h, Algorithms/Complex/gpuComputeComplex.cuh) and
 include/superman_b200.h, with the driver templates instantiated for the
