@@ -184,15 +184,19 @@ __global__ void __launch_bounds__(128) list_units(Problem pb)
 // *list_bin = the lowest bin whose tail (units at or above it) holds
 // at most raw_cap/2 units by bound_walk's count.  One warp; lane l owns bins
 // [16l, 16l + 16) and the tails are lane-local sums joined by a warp scan.
+// The counts are staged in shared memory with coalesced loads first.
 __global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
 {
     constexpr int kPer = kHistBins / 32;
     const int lane = threadIdx.x;
     const unsigned full = 0xffffffffu;
+    __shared__ unsigned s_pc[kHistPadded];
+    for (int b = lane; b < kHistBins; b += 32) s_pc[hist_pad_index(b)] = pb.pre_cnt[b];
+    __syncwarp();
     unsigned long long cn[kPer], cl = 0;
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        cn[i] = pb.pre_cnt[lane * kPer + i];
+        cn[i] = s_pc[hist_pad_index(lane * kPer + i)];
         cl += cn[i];
     }
     unsigned long long sfx = cl;  // inclusive suffix over lanes
