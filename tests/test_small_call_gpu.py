@@ -135,3 +135,13 @@ def test_skip_timing_same_result(spb, n):
         assert abs(u.permanent - t.permanent) <= 1e-15 * abs(t.permanent)
         assert u.kernel_s == 0.0
     assert t.kernel_s > 0.0
+
+
+def test_skip_timing_complex(spb):
+    """skip_timing on the complex entry point: the same value, no device
+    timing."""
+    c = W.haar_block(14, seed=14, N=32)
+    t = spb.perm_complex(c, precision="dd")
+    u = spb.perm_complex(c, precision="dd", skip_timing=1)
+    assert abs(u.permanent - t.permanent) <= 1e-14 * abs(t.permanent)
+    assert u.kernel_s == 0.0 and t.kernel_s > 0.0
