@@ -373,23 +373,23 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
         if (terms >= 2 * wk) {
             for (int d = wl; d < terms; d += 2 * wk) {
                 const int d2 = d + wk;
-                dd p1 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
-                dd p2 = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
+                dd p1 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
+                dd p2 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
                 for (int r = 1; r < n; ++r) {
                     const int k1 = r * terms + d, k2 = r * terms + d2;
                     const dd x = {xw[r], xw[n + r]};
-                    p1 = dd_mul(p1, dd_add(x, dd{s_dh[k1], s_dl[k1]}));
-                    p2 = dd_mul(p2, dd_add(x, dd{s_dh[k2], s_dl[k2]}));
+                    p1 = dd_mul(p1, dd_add_fast(x, dd{s_dh[k1], s_dl[k1]}));
+                    p2 = dd_mul(p2, dd_add_fast(x, dd{s_dh[k2], s_dl[k2]}));
                 }
                 acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p1)) : dd_add(acc, p1);
                 acc = (__popc(d2) & 1) ? dd_add(acc, dd_neg(p2)) : dd_add(acc, p2);
             }
         } else {
             for (int d = wl; d < terms; d += wk) {
-                dd p = dd_add(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
+                dd p = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
                 for (int r = 1; r < n; ++r) {
                     const int k = r * terms + d;
-                    p = dd_mul(p, dd_add(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
+                    p = dd_mul(p, dd_add_fast(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
                 }
                 acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
             }
@@ -456,12 +456,12 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
         dd ar = {0.0, 0.0}, ai = {0.0, 0.0};
         for (int d = wl; d < terms; d += wk) {
             int k = d;
-            dd pr = dd_add(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
-            dd pi = dd_add(dd{xw[2 * n], xw[3 * n]}, dd{dih[k], dil[k]});
+            dd pr = dd_add_fast(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
+            dd pi = dd_add_fast(dd{xw[2 * n], xw[3 * n]}, dd{dih[k], dil[k]});
             for (int r = 1; r < n; ++r) {
                 k = r * terms + d;
-                dd yr = dd_add(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
-                dd yi = dd_add(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
+                dd yr = dd_add_fast(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
+                dd yi = dd_add_fast(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
                 dd nr = dd_add(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
                 dd ni = dd_add(dd_mul(pr, yi), dd_mul(pi, yr));
                 pr = nr;

@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(kSmallCallThreads, 1) small_call_real(Problem 
         for (int d = tid / per; d < terms; d += bd / per) {
             dd p = {1.0, 0.0};
             for (int r = r0; r < r1; ++r)
-                p = dd_mul(p, dd_add(dd{xw[r], xw[N + r]}, dd{s_dh[pos(d, r)], s_dl[pos(d, r)]}));
+                p = dd_mul(p, dd_add_fast(dd{xw[r], xw[N + r]}, dd{s_dh[pos(d, r)], s_dl[pos(d, r)]}));
             for (int off = 1; off < per; off <<= 1) p = dd_mul(p, shfl_xor_dd(p, off));
             if (sub == 0) acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
         }

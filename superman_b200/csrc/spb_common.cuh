@@ -89,6 +89,16 @@ __host__ __device__ __forceinline__ dd dd_add(dd a, dd b)
 
 __host__ __device__ __forceinline__ dd dd_neg(dd a) { return {-a.hi, -a.lo}; }
 
+// a + b left unnormalised: hi = fl(a.hi + b.hi), lo = its rounding error
+// plus both lo words.  About 2^-106 (|a| + |b|) off; 8 operations against 20
+// for dd_add, for a factor that goes straight into dd_mul (which takes an
+// unnormalised operand and returns a normalised product).
+__host__ __device__ __forceinline__ dd dd_add_fast(dd a, dd b)
+{
+    const dd s = two_sum(a.hi, b.hi);
+    return {s.hi, add_rn(s.lo, add_rn(a.lo, b.lo))};
+}
+
 // (a.hi + a.lo) * (b.hi + b.lo) to ~2^-104 relative (Dekker product with FMA).
 __device__ __forceinline__ dd dd_mul(dd a, dd b)
 {
