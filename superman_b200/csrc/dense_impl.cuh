@@ -71,15 +71,28 @@ struct Problem {
     unsigned short* raw_b;         // [raw_cap] its bound bin
 };
 
-// Capacity of the mode-1 list (units); pick_list_bin aims at half of it so
-// that bins computed by the walk and by bound_walk may differ at bin edges.
+// Capacity of the mode-1 list (units).  pick_list_bin aims at kRawTarget,
+// an eighth of it, so that bins computed by the walk and by bound_walk may
+// differ at bin edges; the units the refinement takes (a few hundred to a
+// few thousand from n = 27 to 32) fit that target many times over, and every
+// listed unit costs the walk an append.
 constexpr unsigned long long kRawCap = 1ull << 17;
+constexpr unsigned long long kRawTarget = kRawCap / 8;
 
-// Appends unit u (bound bin b) to the mode-1 list when b >= lbin.
+// Appends unit u (bound bin b) to the mode-1 list when b >= lbin.  The
+// appending lanes of a warp take their slots with one atomic (a leader
+// reserves popc of them), not one each.
 __device__ __forceinline__ void raw_list_add(const Problem& pb, int lbin, unsigned long long u, int b)
 {
-    if (b < lbin) return;
-    const unsigned long long k = atomicAdd(pb.raw_n, 1ull);
+    const unsigned act = __activemask();
+    const bool want = b >= lbin;
+    const unsigned m = __ballot_sync(act, want);
+    if (!want) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(pb.raw_n, (unsigned long long)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const unsigned long long k = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
     if (k < pb.raw_cap) {
         pb.raw_u[k] = u;
         pb.raw_b[k] = (unsigned short)b;

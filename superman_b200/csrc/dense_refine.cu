@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(128) list_units(Problem pb)
 }
 
 // *list_bin = the lowest bin whose tail (units at or above it) holds
-// at most raw_cap/2 units by bound_walk's count.  One warp; lane l owns bins
+// at most kRawTarget units by bound_walk's count.  One warp; lane l owns bins
 // [16l, 16l + 16) and the tails are lane-local sums joined by a warp scan.
 // The counts are staged in shared memory with coalesced loads first.
 __global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
@@ -207,12 +207,12 @@ __global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
     }
     unsigned long long tail = __shfl_down_sync(full, sfx, 1);
     if (lane == 31) tail = 0;
-    const unsigned long long half = pb.raw_cap / 2;
+    const unsigned long long target = kRawTarget;
     int b = kHistBins;
 #pragma unroll
     for (int i = kPer - 1; i >= 0; --i) {
         tail += cn[i];
-        if (tail <= half) b = lane * kPer + i;
+        if (tail <= target) b = lane * kPer + i;
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) b = min(b, __shfl_xor_sync(full, b, d));
