@@ -284,25 +284,31 @@ __device__ __forceinline__ void stage(double* dst, const double* __restrict__ sr
 // Copies `parts` subset-sum tables laid out [q][n][G] (the walks' grouping,
 // q = d / G) into shared memory as [n][terms] (d contiguous per row), so
 // that lanes taking consecutive terms of one row read consecutive words
-// rather than words n*G apart in one bank.  Eight loads in flight per thread.
+// rather than words n*G apart in one bank.  A group of G words is
+// contiguous on both sides, so each thread moves whole groups (one index
+// division per group, not four per word), eight groups in flight.
 __device__ __forceinline__ void stage_rows(double* dst, const double* __restrict__ src, int parts, int n,
                                            int terms, int G)
 {
-    const int per = terms * n, m = parts * per, bd = blockDim.x;
-    for (int i0 = threadIdx.x; i0 < m; i0 += 8 * bd) {
-        double v[8];
+    const int per = terms * n, nq = terms / G, groups = parts * nq * n, bd = blockDim.x;
+    for (int j0 = threadIdx.x; j0 < groups; j0 += 8 * bd) {
+        double v[8][4];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int i = i0 + k * bd;
-            v[k] = i < m ? __ldg(src + i) : 0.0;
+            const int j = j0 + k * bd;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) v[k][g] = (j < groups && g < G) ? __ldg(src + (size_t)j * G + g) : 0.0;
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int i = i0 + k * bd;
-            if (i < m) {
-                const int part = i / per, rem = i % per;
-                const int q = rem / (n * G), rg = rem % (n * G);
-                dst[part * per + (rg / G) * terms + q * G + rg % G] = v[k];
+            const int j = j0 + k * bd;
+            if (j < groups) {
+                // j = (part * nq + q) * n + r
+                const int qr = j % (nq * n), part = j / (nq * n), q = qr / n, r = qr % n;
+                double* d = dst + (size_t)part * per + (size_t)r * terms + q * G;
+#pragma unroll
+                for (int g = 0; g < 4; ++g)
+                    if (g < G) d[g] = v[k][g];
             }
         }
     }
@@ -330,7 +336,8 @@ __device__ __forceinline__ void worker_sync(bool wide)
 
 // A unit is refined by a worker: one warp per unit, or, when there are at
 // most as many units as CTAs, one CTA per unit (the units then spread over
-// more SMs).  A worker's threads take terms; each runs two independent term
+// more SMs).  Units are dealt out CTA by CTA (unit e to CTA e mod grid), so
+// that a few hundred units occupy every SM rather than filling a few.  A worker's threads take terms; each runs two independent term
 // chains at a time when it has two.
 __global__ void __launch_bounds__(512) refine_real(Problem pb)
 {
@@ -350,7 +357,7 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
     double* s_g = s_x + nwarps * 2 * n;  // [nwarps][nq]
     double* s_mt = s_g + nwarps * nq;    // [ntp][n]
     // CTAs without a unit skip the tables (they still join the grid reduction)
-    if ((unsigned long long)blockIdx.x * nwk < count) {
+    if ((unsigned long long)blockIdx.x < count) {
         stage_rows(s_dh, pb.de_hi, 1, n, terms, G);  // [n][terms]
         stage_rows(s_dl, pb.de_lo, 1, n, terms, G);
         stage(s_mt, pb.mt, ntp * n);
@@ -359,7 +366,7 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
     double* xw = s_x + wid * 2 * n;
     double* gw = s_g + wid * nq;
     dd corr = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)blockIdx.x * nwk + wid; e < count;
+    for (unsigned long long e = (unsigned long long)wid * gridDim.x + blockIdx.x; e < count;
          e += (unsigned long long)gridDim.x * nwk) {
         if (pb.list_x) {
             const double* src = pb.list_x + e * (2 * n);
@@ -427,7 +434,7 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
     double* s_g = s_x + nwarps * 4 * n;   // [nwarps][2*nq]
     double* s_mt = s_g + nwarps * 2 * nq; // [2][ntp][n]
     // CTAs without a unit skip the tables (they still join the grid reduction)
-    if ((unsigned long long)blockIdx.x * nwk < count) {
+    if ((unsigned long long)blockIdx.x < count) {
         stage_rows(s_dh, pb.de_hi, 2, n, terms, G);  // [2][n][terms]
         stage_rows(s_dl, pb.de_lo, 2, n, terms, G);
         stage(s_mt, pb.mt, 2 * ntp * n);
@@ -440,7 +447,7 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
     double* xw = s_x + wid * 4 * n;  // xr hi, xr lo, xi hi, xi lo
     double* gw = s_g + wid * 2 * nq;
     dd corr_r = {0.0, 0.0}, corr_i = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)blockIdx.x * nwk + wid; e < count;
+    for (unsigned long long e = (unsigned long long)wid * gridDim.x + blockIdx.x; e < count;
          e += (unsigned long long)gridDim.x * nwk) {
         if (pb.list_x) {
             const double* src = pb.list_x + e * (4 * n);
