@@ -469,8 +469,10 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
                 k = r * terms + d;
                 dd yr = dd_add_fast(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
                 dd yi = dd_add_fast(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
-                dd nr = dd_add(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
-                dd ni = dd_add(dd_mul(pr, yi), dd_mul(pi, yr));
+                // the products' sums unnormalised (dd_add_fast: about 2^-106 of
+                // |pr yr| + |pi yi| off, far inside what the refinement corrects)
+                dd nr = dd_add_fast(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
+                dd ni = dd_add_fast(dd_mul(pr, yi), dd_mul(pi, yr));
                 pr = nr;
                 pi = ni;
             }
