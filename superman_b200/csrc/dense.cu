@@ -71,13 +71,19 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
         }
     }
     __syncthreads();
-    // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in [0.5, 1).
-    for (int r = tid; r < n; r += bd) {
+    const int lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
+    // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in
+    //    [0.5, 1).  A warp per row (fmax does not depend on the order).
+    for (int r = wid; r < n; r += nw) {
         double mx = 0.0;
-        for (int j = 0; j < n * c; ++j) mx = fmax(mx, fabs(s_as[r * n * c + j]));
-        int e = 0;
-        if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
-        s_exp[r] = e;
+        for (int j = lane; j < n * c; j += 32) mx = fmax(mx, fabs(s_as[r * n * c + j]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        if (lane == 0) {
+            int e = 0;
+            if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+            s_exp[r] = e;
+        }
     }
     __syncthreads();
     for (int idx = tid; idx < n * n * c; idx += bd) {
@@ -92,41 +98,67 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
         for (int r = 0; r < n; ++r) es += s_exp[r];
         *pb.exp_sum = es;
     }
-    // 2. NW start vector in double-double: x0_r = a'_{r,n-1} - rowsum'_r / 2.
-    for (int rr = tid; rr < n * c; rr += bd) {
-        int r = rr / c, part = rr % c;
-        dd s = {0.0, 0.0};
-        for (int j = 0; j < n; ++j) s = dd_add_d(s, s_as[(r * n + j) * c + part]);
-        dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
-        dd x = dd_add_d(h, s_as[(r * n + (n - 1)) * c + part]);
-        pb.x0_hi[part * n + r] = x.hi;
-        pb.x0_lo[part * n + r] = x.lo;
-    }
-    // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per part:
-    //    the double-double sum of the selected columns added in ascending
-    //    order.  Built level by level: with k the highest bit of d,
-    //    DE[d] = DE[d - 2^k] + a_k, the same operations in the same order.
-    auto de_pos = [&](int part, int d, int r) {
-        return (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
-    };
-    for (int idx = tid; idx < n * c; idx += bd) {
-        const size_t pos = de_pos(idx / n, 0, idx % n);
-        dh[pos] = 0.0;
-        dl[pos] = 0.0;
-        if (pb.de32) pb.de32[pos] = 0.0f;
-    }
-    for (int k = 0; k < w; ++k) {
-        __syncthreads();  // level k reads the entries of levels < k
-        const int half = 1 << k;
-        for (int idx = tid; idx < half * n * c; idx += bd) {
-            const int part = idx / (half * n), rem = idx % (half * n);
-            const int d = half + rem / n, r = rem % n;
-            const size_t from = de_pos(part, d - half, r);
-            const dd s = dd_add_d(dd{dh[from], dl[from]}, s_as[(r * n + k) * c + part]);
-            const size_t pos = de_pos(part, d, r);
-            dh[pos] = s.hi;
-            dl[pos] = s.lo;
-            if (pb.de32) pb.de32[pos] = __double2float_rn(s.hi);
+    // 2 and 3 side by side: the NW start vector on the last warps (one row
+    // and part per lane, n dependent adds), the subset-sum tables on the
+    // other warps.
+    const int xwarps = (n * c + 31) / 32, dwarps = nw - xwarps;  // dwarps >= 1 with 512 threads
+    if (wid >= dwarps) {
+        // 2. NW start vector in double-double: x0_r = a'_{r,n-1} - rowsum'_r / 2.
+        const int rr = (wid - dwarps) * 32 + lane;
+        if (rr < n * c) {
+            const int r = rr / c, part = rr % c;
+            dd s = {0.0, 0.0};
+            for (int j = 0; j < n; ++j) s = dd_add_d(s, s_as[(r * n + j) * c + part]);
+            dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
+            dd x = dd_add_d(h, s_as[(r * n + (n - 1)) * c + part]);
+            pb.x0_hi[part * n + r] = x.hi;
+            pb.x0_lo[part * n + r] = x.lo;
+        }
+    } else {
+        // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per
+        //    part: the double-double sum of the selected columns added in
+        //    ascending order.  Built level by level per (part, row): with k
+        //    the highest bit of d, DE[d] = DE[d - 2^k] + a_k, the same
+        //    operations in the same order; a warp takes two rows side by
+        //    side, its lanes a level's entries, and meets at a warp barrier.
+        auto de_pos = [&](int part, int d, int r) {
+            return (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
+        };
+        for (int q0 = wid; q0 < n * c; q0 += 2 * dwarps) {
+            const int q1 = q0 + dwarps;  // pairs q = part * n + r
+            const bool two = q1 < n * c;
+            const int pa0 = q0 / n, r0 = q0 % n, pa1 = two ? q1 / n : 0, r1 = two ? q1 % n : 0;
+            if (lane == 0) {
+                dh[de_pos(pa0, 0, r0)] = 0.0;
+                dl[de_pos(pa0, 0, r0)] = 0.0;
+                if (pb.de32) pb.de32[de_pos(pa0, 0, r0)] = 0.0f;
+                if (two) {
+                    dh[de_pos(pa1, 0, r1)] = 0.0;
+                    dl[de_pos(pa1, 0, r1)] = 0.0;
+                    if (pb.de32) pb.de32[de_pos(pa1, 0, r1)] = 0.0f;
+                }
+            }
+            for (int k = 0; k < w; ++k) {
+                __syncwarp();  // level k reads the entries of levels < k
+                const int half = 1 << k;
+                const double a0 = s_as[(r0 * n + k) * c + pa0];
+                const double a1 = two ? s_as[(r1 * n + k) * c + pa1] : 0.0;
+                for (int e = lane; e < half; e += 32) {
+                    const size_t f0 = de_pos(pa0, e, r0), t0 = de_pos(pa0, half + e, r0);
+                    const dd v0 = dd_add_d(dd{dh[f0], dl[f0]}, a0);
+                    if (two) {
+                        const size_t f1 = de_pos(pa1, e, r1), t1 = de_pos(pa1, half + e, r1);
+                        const dd v1 = dd_add_d(dd{dh[f1], dl[f1]}, a1);
+                        dh[t1] = v1.hi;
+                        dl[t1] = v1.lo;
+                        if (pb.de32) pb.de32[t1] = __double2float_rn(v1.hi);
+                    }
+                    dh[t0] = v0.hi;
+                    dl[t0] = v0.lo;
+                    if (pb.de32) pb.de32[t0] = __double2float_rn(v0.hi);
+                }
+            }
+            __syncwarp();
         }
     }
     // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
