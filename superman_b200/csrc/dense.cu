@@ -52,7 +52,7 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
     __shared__ int s_exp[kMaxN];
     extern __shared__ double s_as[];  // [n][n][c], row-scaled after step 1; then the table
     const int terms = 1 << w;
-    double* dh = smem_tables ? s_as + n * n * c : pb.de_hi;  // [c][terms/G][n][G]
+    double* dh = smem_tables ? s_as + ((n * n * c + 1) & ~1) : pb.de_hi;  // [c][terms/G][n][G]
     double* dl = smem_tables ? dh + (size_t)c * terms * n : pb.de_lo;
 
     for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
@@ -101,6 +101,10 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
     // 2 and 3 side by side: the NW start vector on the last warps (one row
     // and part per lane, n dependent adds), the subset-sum tables on the
     // other warps.
+    // G is 1, 2 or 4: table entry d of row r (part p) sits at
+    // p*terms*n + r*G + (d >> lg)*n*G + (d & (G-1)).
+    const int lg = G == 4 ? 2 : (G == 2 ? 1 : 0), gm = G - 1, ng = n * G;
+    auto off = [&](int d) { return (d >> lg) * ng + (d & gm); };
     const int xwarps = (n * c + 31) / 32, dwarps = nw - xwarps;  // dwarps >= 1 with 512 threads
     if (wid >= dwarps) {
         // 2. NW start vector in double-double: x0_r = a'_{r,n-1} - rowsum'_r / 2.
@@ -121,21 +125,19 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
         //    the highest bit of d, DE[d] = DE[d - 2^k] + a_k, the same
         //    operations in the same order; a warp takes two rows side by
         //    side, its lanes a level's entries, and meets at a warp barrier.
-        auto de_pos = [&](int part, int d, int r) {
-            return (size_t)part * terms * n + ((size_t)(d / G) * n + r) * G + (d % G);
-        };
         for (int q0 = wid; q0 < n * c; q0 += 2 * dwarps) {
             const int q1 = q0 + dwarps;  // pairs q = part * n + r
             const bool two = q1 < n * c;
             const int pa0 = q0 / n, r0 = q0 % n, pa1 = two ? q1 / n : 0, r1 = two ? q1 % n : 0;
+            const size_t b0 = (size_t)pa0 * terms * n + r0 * G, b1 = (size_t)pa1 * terms * n + r1 * G;
             if (lane == 0) {
-                dh[de_pos(pa0, 0, r0)] = 0.0;
-                dl[de_pos(pa0, 0, r0)] = 0.0;
-                if (pb.de32) pb.de32[de_pos(pa0, 0, r0)] = 0.0f;
+                dh[b0] = 0.0;
+                dl[b0] = 0.0;
+                if (pb.de32) pb.de32[b0] = 0.0f;
                 if (two) {
-                    dh[de_pos(pa1, 0, r1)] = 0.0;
-                    dl[de_pos(pa1, 0, r1)] = 0.0;
-                    if (pb.de32) pb.de32[de_pos(pa1, 0, r1)] = 0.0f;
+                    dh[b1] = 0.0;
+                    dl[b1] = 0.0;
+                    if (pb.de32) pb.de32[b1] = 0.0f;
                 }
             }
             for (int k = 0; k < w; ++k) {
@@ -144,35 +146,45 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
                 const double a0 = s_as[(r0 * n + k) * c + pa0];
                 const double a1 = two ? s_as[(r1 * n + k) * c + pa1] : 0.0;
                 for (int e = lane; e < half; e += 32) {
-                    const size_t f0 = de_pos(pa0, e, r0), t0 = de_pos(pa0, half + e, r0);
-                    const dd v0 = dd_add_d(dd{dh[f0], dl[f0]}, a0);
+                    const int fo = off(e), to = off(half + e);
+                    const dd v0 = dd_add_d(dd{dh[b0 + fo], dl[b0 + fo]}, a0);
                     if (two) {
-                        const size_t f1 = de_pos(pa1, e, r1), t1 = de_pos(pa1, half + e, r1);
-                        const dd v1 = dd_add_d(dd{dh[f1], dl[f1]}, a1);
-                        dh[t1] = v1.hi;
-                        dl[t1] = v1.lo;
-                        if (pb.de32) pb.de32[t1] = __double2float_rn(v1.hi);
+                        const dd v1 = dd_add_d(dd{dh[b1 + fo], dl[b1 + fo]}, a1);
+                        dh[b1 + to] = v1.hi;
+                        dl[b1 + to] = v1.lo;
+                        if (pb.de32) pb.de32[b1 + to] = __double2float_rn(v1.hi);
                     }
-                    dh[t0] = v0.hi;
-                    dl[t0] = v0.lo;
-                    if (pb.de32) pb.de32[t0] = __double2float_rn(v0.hi);
+                    dh[b0 + to] = v0.hi;
+                    dl[b0 + to] = v0.lo;
+                    if (pb.de32) pb.de32[b0 + to] = __double2float_rn(v0.hi);
                 }
             }
             __syncwarp();
         }
     }
     // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
-    //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|.
-    //     The complex maximum spreads the (row, d) pairs over all threads; the
-    //     bit patterns of non-negative doubles order like the values.
-    __shared__ unsigned long long s_bmax[kMaxN];
-    for (int r = tid; r < n; r += bd) s_bmax[r] = 0ull;
+    //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|,
+    //     a warp per row over d; the bit patterns of non-negative doubles
+    //     order like the values.
     __syncthreads();  // the complex bound and the write-out read the table written above
-    if (smem_tables)
-        for (int i = tid; i < c * terms * n; i += bd) {
-            pb.de_hi[i] = dh[i];
-            pb.de_lo[i] = dl[i];
+    if (smem_tables) {
+        const int cnt = c * terms * n;
+        if (cnt & 1) {  // n = 1: a table of one entry
+            for (int i = tid; i < cnt; i += bd) {
+                pb.de_hi[i] = dh[i];
+                pb.de_lo[i] = dl[i];
+            }
+        } else {  // dh and dl = dh + cnt start on 16-byte boundaries
+            const double2* sh = reinterpret_cast<const double2*>(dh);
+            const double2* sl = reinterpret_cast<const double2*>(dl);
+            double2* gh = reinterpret_cast<double2*>(pb.de_hi);
+            double2* gl = reinterpret_cast<double2*>(pb.de_lo);
+            for (int i = tid; i < cnt / 2; i += bd) {
+                gh[i] = sh[i];
+                gl[i] = sl[i];
+            }
         }
+    }
     if (c == 1) {
         for (int r = tid; r < n; r += bd) {
             double lo = 0.0, hi = 0.0;
@@ -184,14 +196,17 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
             pb.bnd[n + r] = hi;
         }
     } else {
-        for (int idx = tid; idx < terms * n; idx += bd) {
-            const int r = idx % n, d = idx / n;
-            const size_t pos = ((size_t)(d / G) * n + r) * G + (d % G);
-            const double m = hypot(dh[pos], dh[(size_t)terms * n + pos]);
-            atomicMax(&s_bmax[r], (unsigned long long)__double_as_longlong(m));
+        for (int r = wid; r < n; r += nw) {
+            unsigned long long mx = 0ull;
+            for (int d = lane; d < terms; d += 32) {
+                const size_t pos = (size_t)r * G + off(d);
+                const double m = hypot(dh[pos], dh[(size_t)terms * n + pos]);
+                mx = max(mx, (unsigned long long)__double_as_longlong(m));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) pb.bnd[r] = __longlong_as_double((long long)mx) * (1.0 + 0x1p-50);
         }
-        __syncthreads();
-        for (int r = tid; r < n; r += bd) pb.bnd[r] = __longlong_as_double((long long)s_bmax[r]) * (1.0 + 0x1p-50);
     }
     // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
     const int ntop = n - 1 - w;
@@ -213,7 +228,9 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
 namespace spb {
 namespace dense {
 
-size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (size_t)n * n * comps; }
+// The staged matrix, rounded up to an even count of doubles (the tables that
+// may follow it are copied out in 16-byte pairs).
+size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (((size_t)n * n * comps + 1) & ~(size_t)1); }
 
 // The fused small-matrix call (small_call.cu).
 constexpr int kSmallCallMaxN = 26;
