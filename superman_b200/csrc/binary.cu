@@ -90,12 +90,19 @@ static int run(const uint8_t* a, int n, const spb_options* opt_in, uint32_t* lim
     int threads = opt.threads_per_block > 0 ? (opt.threads_per_block / 32) * 32 : tmax;
     if (threads > tmax) threads = tmax;
     if (threads < 32) threads = 32;
-    int blocks = opt.blocks > 0 ? opt.blocks : ctx->sm_count;
+    const size_t smem = sizeof(int) * terms * n + align_up((size_t)(ntop > 0 ? ntop : 1) * n, 16);
+    // Default grid: every CTA that fits resident at once (two per SM where
+    // the registers allow, e.g. 256 threads at 128 registers).
+    int blocks = opt.blocks;
+    if (blocks <= 0) {
+        int per_sm = 0;
+        if ((st = launch_binary(pb, 0, threads, smem, stream, &per_sm)) != SPB_OK) return out->status = st;
+        blocks = ctx->sm_count * (per_sm > 0 ? per_sm : 1);
+    }
     unsigned long long max_blocks = (pb.units + threads - 1) / threads;
     if ((unsigned long long)blocks > max_blocks) blocks = (int)max_blocks;
     if (blocks < 1) blocks = 1;
     pb.grid = blocks;
-    const size_t smem = sizeof(int) * terms * n + align_up((size_t)(ntop > 0 ? ntop : 1) * n, 16);
 
     // host-built tables: x'_r = 2 a_{r,n-1} - rowsum_r, doubled low-column
     // counts, doubled high columns

@@ -309,7 +309,9 @@ __global__ void __launch_bounds__(bin_max_threads(N, L), 1) walk_binary(Problem 
     }
 }
 
-int launch_binary(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s);
+// Launches walk_binary<pb.n, pb.limbs>; with per_sm set, launches nothing
+// and stores the CTAs per SM that the launch shape allows.
+int launch_binary(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s, int* per_sm = nullptr);
 
 }  // namespace binary
 }  // namespace spb

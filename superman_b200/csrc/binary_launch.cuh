@@ -9,8 +9,10 @@
 namespace spb {
 namespace binary {
 
+// With per_sm set, launches nothing and stores how many CTAs of `threads`
+// threads and `smem` bytes fit on one SM.
 template <int N, int L>
-int launch_bin_n(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s)
+int launch_bin_n(const Problem& pb, int blocks, int threads, size_t smem, cudaStream_t s, int* per_sm)
 {
     static std::once_flag once[64];
     static cudaError_t attr_err[64];
@@ -27,6 +29,10 @@ int launch_bin_n(const Problem& pb, int blocks, int threads, size_t smem, cudaSt
                                                       optin - (int)fa.sharedSizeBytes);
     });
     SPB_CUDA_TRY(attr_err[dev & 63]);
+    if (per_sm) {
+        SPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, walk_binary<N, L>, threads, smem));
+        return SPB_OK;
+    }
     walk_binary<N, L><<<blocks, threads, smem, s>>>(pb);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
