@@ -40,182 +40,175 @@ namespace spb {
 namespace dense {
 
 // ------------------------------------------------------------ setup kernel --
-// One CTA builds every table the walk kernels read.  The matrix is staged in
-// shared memory (dynamic, n*n*comps doubles: setup_smem_bytes), so the table
-// builds below read it at shared-memory latency.  With smem_tables the
-// subset-sum table is also built in shared memory (each level reads the
-// levels below it) and written out once at the end.
-__global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int smem_tables)
+// Builds every table the walk kernels read, one CTA per row r (every value
+// below depends on its own row only, apart from the exponent sum, which
+// CTA 0 adds up).  Row r is staged in shared memory (CTA 0 stages the whole
+// matrix, n*n*comps doubles, for the exponents of every row).
+// Per part, one warp builds the row's subset sums DE[d][r] level by level
+// behind warp barriers (in shared memory with smem_tables, else in place in
+// the global table), another forms the NW start value, and the CTA then
+// writes the tables out, the row's bound and its high columns.
+//   4 warps: 0, 1 tables (part 0, 1), 2 start values, 3 high columns.
+__global__ void __launch_bounds__(128) setup_kernel(Problem pb, const double* __restrict__ a_in, int smem_tables)
 {
     const int n = pb.n, c = pb.comps, w = pb.w, G = pb.g;
-    const int tid = threadIdx.x, bd = blockDim.x;
-    __shared__ int s_exp[kMaxN];
-    extern __shared__ double s_as[];  // [n][n][c], row-scaled after step 1; then the table
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5, r = blockIdx.x;
     const int terms = 1 << w;
-    double* dh = smem_tables ? s_as + ((n * n * c + 1) & ~1) : pb.de_hi;  // [c][terms/G][n][G]
-    double* dl = smem_tables ? dh + (size_t)c * terms * n : pb.de_lo;
+    __shared__ int s_eall[kMaxN];
+    // CTA 0 stages the whole matrix (it also adds up every row's exponent),
+    // the others their row: row r is s_row[0 .. n*c) either way
+    extern __shared__ __align__(16) double s_row[];  // [rows][n][c], scaled after step 1; then [c][terms] hi, lo
+    double* th = s_row + ((n * n * c + 1) & ~1);
+    double* tl = th + (size_t)c * terms;
+    const int nst = r == 0 ? n : 1;
 
-    for (int idx = tid; idx < n * n * c; idx += bd) s_as[idx] = a_in[idx];
     // 0. What the later kernels of the call accumulate into starts at zero.
-    if (tid < 4) pb.ticket[tid] = 0u;
-    if (pb.f32 && tid == 0) pb.rb->err = 0.0;  // the FP32 walk's sum of squared terms
-    if (pb.mode != 0) {
-        for (int i = tid; i < kHistBins; i += bd) {
-            pb.hist_s2[i] = 0.0;
-            pb.hist_cnt[i] = 0ull;
-            pb.pre_cnt[i] = 0u;
-        }
-        if (tid == 0) {
-            *pb.raw_n = 0ull;
-            *pb.list_bin = pb.list_bin_init;
+    if (r == 0) {
+        if (tid < 4) pb.ticket[tid] = 0u;
+        if (pb.f32 && tid == 0) pb.rb->err = 0.0;  // the FP32 walk's sum of squared terms
+        if (pb.mode != 0) {
+            for (int i = tid; i < kHistBins; i += bd) {
+                pb.hist_s2[i] = 0.0;
+                pb.hist_cnt[i] = 0ull;
+                pb.pre_cnt[i] = 0u;
+            }
+            if (tid == 0) {
+                *pb.raw_n = 0ull;
+                *pb.list_bin = pb.list_bin_init;
+            }
         }
     }
+    for (int i = tid; i < nst * n * c; i += bd) s_row[i] = a_in[(size_t)r * n * c + i];
     __syncthreads();
-    const int lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
-    // 1. Row exponents: scale row r by 2^-e_r so that max |a_rj| lies in
-    //    [0.5, 1).  A warp per row (fmax does not depend on the order).
-    for (int r = wid; r < n; r += nw) {
+    // 1. Row exponents: scale row q by 2^-e_q so that its largest |a_qj| lies
+    //    in [0.5, 1); a warp per staged row (fmax does not depend on the
+    //    order).  CTA 0 writes their sum.
+    for (int q = wid; q < nst; q += bd >> 5) {
         double mx = 0.0;
-        for (int j = lane; j < n * c; j += 32) mx = fmax(mx, fabs(s_as[r * n * c + j]));
+        for (int j = lane; j < n * c; j += 32) mx = fmax(mx, fabs(s_row[q * n * c + j]));
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
         if (lane == 0) {
             int e = 0;
             if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
-            s_exp[r] = e;
+            s_eall[q] = e;
         }
     }
     __syncthreads();
-    for (int idx = tid; idx < n * n * c; idx += bd) {
-        int r = idx / (n * c);
-        const double v = ldexp(s_as[idx], -s_exp[r]);
-        s_as[idx] = v;
-        pb.as[idx] = v;
-    }
-    __syncthreads();
-    if (tid == 0) {
+    if (r == 0 && wid == 0) {
         int es = 0;
-        for (int r = 0; r < n; ++r) es += s_exp[r];
-        *pb.exp_sum = es;
+        for (int q = lane; q < n; q += 32) es += s_eall[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) es += __shfl_xor_sync(0xffffffffu, es, off);
+        if (lane == 0) *pb.exp_sum = es;
     }
-    // 2 and 3 side by side: the NW start vector on the last warps (one row
-    // and part per lane, n dependent adds), the subset-sum tables on the
-    // other warps.
-    // G is 1, 2 or 4: table entry d of row r (part p) sits at
-    // p*terms*n + r*G + (d >> lg)*n*G + (d & (G-1)).
-    const int lg = G == 4 ? 2 : (G == 2 ? 1 : 0), gm = G - 1, ng = n * G;
-    auto off = [&](int d) { return (d >> lg) * ng + (d & gm); };
-    const int xwarps = (n * c + 31) / 32, dwarps = nw - xwarps;  // dwarps >= 1 with 512 threads
-    if (wid >= dwarps) {
-        // 2. NW start vector in double-double: x0_r = a'_{r,n-1} - rowsum'_r / 2.
-        const int rr = (wid - dwarps) * 32 + lane;
-        if (rr < n * c) {
-            const int r = rr / c, part = rr % c;
-            dd s = {0.0, 0.0};
-            for (int j = 0; j < n; ++j) s = dd_add_d(s, s_as[(r * n + j) * c + part]);
-            dd h = {-0.5 * s.hi, -0.5 * s.lo};  // exact halving
-            dd x = dd_add_d(h, s_as[(r * n + (n - 1)) * c + part]);
-            pb.x0_hi[part * n + r] = x.hi;
-            pb.x0_lo[part * n + r] = x.lo;
-        }
-    } else {
-        // 3. Low-column subset sums DE[d][r], grouped [d/G][r][d%G], per
-        //    part: the double-double sum of the selected columns added in
-        //    ascending order.  Built level by level per (part, row): with k
-        //    the highest bit of d, DE[d] = DE[d - 2^k] + a_k, the same
-        //    operations in the same order; a warp takes two rows side by
-        //    side, its lanes a level's entries, and meets at a warp barrier.
-        for (int q0 = wid; q0 < n * c; q0 += 2 * dwarps) {
-            const int q1 = q0 + dwarps;  // pairs q = part * n + r
-            const bool two = q1 < n * c;
-            const int pa0 = q0 / n, r0 = q0 % n, pa1 = two ? q1 / n : 0, r1 = two ? q1 % n : 0;
-            const size_t b0 = (size_t)pa0 * terms * n + r0 * G, b1 = (size_t)pa1 * terms * n + r1 * G;
+    const int er = s_eall[0];
+    for (int i = tid; i < n * c; i += bd) {
+        const double v = ldexp(s_row[i], -er);
+        s_row[i] = v;
+        pb.as[(size_t)r * n * c + i] = v;
+    }
+    __syncthreads();
+    // entry d of row r, part p, in the global table [c][terms/G][n][G]
+    auto gpos = [&](int p, int d) {
+        return (size_t)p * terms * n + (size_t)(d / G) * n * G + (size_t)r * G + (d % G);
+    };
+    if (wid < c) {
+        // 3. Low-column subset sums of part p = wid: the double-double sum
+        //    of the selected columns added in ascending order, level by
+        //    level: with k the highest bit of d, DE[d] = DE[d - 2^k] + a_k.
+        const int p = wid;
+        double* hh = th + (size_t)p * terms;
+        double* ll = tl + (size_t)p * terms;
+        if (smem_tables) {
             if (lane == 0) {
-                dh[b0] = 0.0;
-                dl[b0] = 0.0;
-                if (pb.de32) pb.de32[b0] = 0.0f;
-                if (two) {
-                    dh[b1] = 0.0;
-                    dl[b1] = 0.0;
-                    if (pb.de32) pb.de32[b1] = 0.0f;
-                }
+                hh[0] = 0.0;
+                ll[0] = 0.0;
             }
             for (int k = 0; k < w; ++k) {
                 __syncwarp();  // level k reads the entries of levels < k
                 const int half = 1 << k;
-                const double a0 = s_as[(r0 * n + k) * c + pa0];
-                const double a1 = two ? s_as[(r1 * n + k) * c + pa1] : 0.0;
+                const double ak = s_row[k * c + p];
                 for (int e = lane; e < half; e += 32) {
-                    const int fo = off(e), to = off(half + e);
-                    const dd v0 = dd_add_d(dd{dh[b0 + fo], dl[b0 + fo]}, a0);
-                    if (two) {
-                        const dd v1 = dd_add_d(dd{dh[b1 + fo], dl[b1 + fo]}, a1);
-                        dh[b1 + to] = v1.hi;
-                        dl[b1 + to] = v1.lo;
-                        if (pb.de32) pb.de32[b1 + to] = __double2float_rn(v1.hi);
-                    }
-                    dh[b0 + to] = v0.hi;
-                    dl[b0 + to] = v0.lo;
-                    if (pb.de32) pb.de32[b0 + to] = __double2float_rn(v0.hi);
+                    const dd v = dd_add_d(dd{hh[e], ll[e]}, ak);
+                    hh[half + e] = v.hi;
+                    ll[half + e] = v.lo;
                 }
             }
-            __syncwarp();
-        }
-    }
-    // 3b. Per-row range of DE over d, for the unit bounds of the refinement:
-    //     real [sum_j min(0,a'_rj), sum_j max(0,a'_rj)]; complex max_d |DE[d][r]|,
-    //     a warp per row over d; the bit patterns of non-negative doubles
-    //     order like the values.
-    __syncthreads();  // the complex bound and the write-out read the table written above
-    if (smem_tables) {
-        const int cnt = c * terms * n;
-        if (cnt & 1) {  // n = 1: a table of one entry
-            for (int i = tid; i < cnt; i += bd) {
-                pb.de_hi[i] = dh[i];
-                pb.de_lo[i] = dl[i];
+        } else {
+            if (lane == 0) {
+                pb.de_hi[gpos(p, 0)] = 0.0;
+                pb.de_lo[gpos(p, 0)] = 0.0;
             }
-        } else {  // dh and dl = dh + cnt start on 16-byte boundaries
-            const double2* sh = reinterpret_cast<const double2*>(dh);
-            const double2* sl = reinterpret_cast<const double2*>(dl);
-            double2* gh = reinterpret_cast<double2*>(pb.de_hi);
-            double2* gl = reinterpret_cast<double2*>(pb.de_lo);
-            for (int i = tid; i < cnt / 2; i += bd) {
-                gh[i] = sh[i];
-                gl[i] = sl[i];
+            for (int k = 0; k < w; ++k) {
+                __syncwarp();
+                const int half = 1 << k;
+                const double ak = s_row[k * c + p];
+                for (int e = lane; e < half; e += 32) {
+                    const size_t f = gpos(p, e), t = gpos(p, half + e);
+                    const dd v = dd_add_d(dd{pb.de_hi[f], pb.de_lo[f]}, ak);
+                    pb.de_hi[t] = v.hi;
+                    pb.de_lo[t] = v.lo;
+                }
             }
         }
-    }
-    if (c == 1) {
-        for (int r = tid; r < n; r += bd) {
+    } else if (wid == 2) {
+        // 2. NW start value in double-double: x0 = a'_{r,n-1} - rowsum'_r / 2.
+        if (lane < c) {
+            const int p = lane;
+            dd sm = {0.0, 0.0};
+            for (int j = 0; j < n; ++j) sm = dd_add_d(sm, s_row[j * c + p]);
+            dd h = {-0.5 * sm.hi, -0.5 * sm.lo};  // exact halving
+            dd x = dd_add_d(h, s_row[(n - 1) * c + p]);
+            pb.x0_hi[p * n + r] = x.hi;
+            pb.x0_lo[p * n + r] = x.lo;
+        }
+    } else if (wid == 3) {
+        // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
+        const int ntop = n - 1 - w;
+        for (int i = lane; i < ntop * c; i += 32) {
+            const int p = i / ntop, j = i % ntop;
+            pb.mt[((size_t)p * ntop + j) * n + r] = s_row[(w + j) * c + p];
+        }
+        // real row bound [sum_j min(0,a'_rj), sum_j max(0,a'_rj)] over the low columns
+        if (c == 1 && lane == 0) {
             double lo = 0.0, hi = 0.0;
             for (int j = 0; j < w; ++j) {
-                double v = s_as[r * n + j];
+                const double v = s_row[j];
                 if (v < 0.0) lo += v; else hi += v;
             }
             pb.bnd[r] = lo;
             pb.bnd[n + r] = hi;
         }
-    } else {
-        for (int r = wid; r < n; r += nw) {
-            unsigned long long mx = 0ull;
-            for (int d = lane; d < terms; d += 32) {
-                const size_t pos = (size_t)r * G + off(d);
-                const double m = hypot(dh[pos], dh[(size_t)terms * n + pos]);
-                mx = max(mx, (unsigned long long)__double_as_longlong(m));
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            if (lane == 0) pb.bnd[r] = __longlong_as_double((long long)mx) * (1.0 + 0x1p-50);
-        }
     }
-    // 4. High columns, column-major: mt[part][j][r] = a'_{r, w+j}.
-    const int ntop = n - 1 - w;
-    for (int idx = tid; idx < ntop * n * c; idx += bd) {
-        int part = idx / (ntop * n);
-        int rem = idx % (ntop * n);
-        int j = rem / n, r = rem % n;
-        pb.mt[idx] = s_as[(r * n + (w + j)) * c + part];
-        (void)part;
+    __syncthreads();
+    // write-out of the tables (the row's entries sit in runs of G), and the
+    // FP32 copy of the hi words for the FP32-product walk
+    if (smem_tables)
+        for (int i = tid; i < c * terms; i += bd) {
+            const int p = i / terms, d = i % terms;
+            const size_t t = gpos(p, d);
+            pb.de_hi[t] = th[i];
+            pb.de_lo[t] = tl[i];
+        }
+    if (pb.de32)
+        for (int i = tid; i < c * terms; i += bd) {
+            const int p = i / terms, d = i % terms;
+            const size_t t = gpos(p, d);
+            pb.de32[t] = __double2float_rn(smem_tables ? th[i] : pb.de_hi[t]);
+        }
+    // complex row bound: max_d |DE[d][r]|, a warp's maximum over d (the bit
+    // patterns of non-negative doubles order like the values)
+    if (c == 2 && wid == 0) {
+        unsigned long long mx = 0ull;
+        for (int d = lane; d < terms; d += 32) {
+            const double re = smem_tables ? th[d] : pb.de_hi[gpos(0, d)];
+            const double im = smem_tables ? th[terms + d] : pb.de_hi[gpos(1, d)];
+            mx = max(mx, (unsigned long long)__double_as_longlong(hypot(re, im)));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) pb.bnd[r] = __longlong_as_double((long long)mx) * (1.0 + 0x1p-50);
     }
 }
 
@@ -228,8 +221,8 @@ __global__ void setup_kernel(Problem pb, const double* __restrict__ a_in, int sm
 namespace spb {
 namespace dense {
 
-// The staged matrix, rounded up to an even count of doubles (the tables that
-// may follow it are copied out in 16-byte pairs).
+// The staged matrix (CTA 0 stages all of it), rounded up to an even count of
+// doubles (a row's tables follow it on a 16-byte boundary).
 size_t setup_smem_bytes(int n, int comps) { return sizeof(double) * (((size_t)n * n * comps + 1) & ~(size_t)1); }
 
 // The fused small-matrix call (small_call.cu).
@@ -241,9 +234,9 @@ int launch_small_call_graph(DeviceContext* ctx, const Problem& pb, const double*
                             int blocks, int threads, Readback* rb_host, bool timed, cudaStream_t s,
                             bool* launched);
 
-// The staged matrix (up to 63*63*2 doubles, 63.5 KB) plus, when it fits, the
-// subset-sum table: the setup kernel's dynamic shared-memory limit is raised to
-// the maximum once per device (which also loads the kernel); *limit receives it.
+// The staged matrix plus, when they fit, one row's subset-sum tables: the setup
+// kernel's dynamic shared-memory limit is raised to the maximum once per
+// device (which also loads the kernel); *limit receives it.
 int prepare_setup(int* limit)
 {
     static std::mutex mu;
@@ -270,9 +263,9 @@ int launch_setup(const Problem& pb, const double* d_a, cudaStream_t s)
     int st = prepare_setup(&limit);
     if (st != SPB_OK) return st;
     const size_t base = setup_smem_bytes(pb.n, pb.comps);
-    const size_t tables = sizeof(double) * 2 * (size_t)pb.comps * ((size_t)1 << pb.w) * pb.n;
+    const size_t tables = sizeof(double) * 2 * (size_t)pb.comps * ((size_t)1 << pb.w);  // one row's
     const int smem_tables = base + tables <= (size_t)limit ? 1 : 0;
-    setup_kernel<<<1, 512, base + (smem_tables ? tables : 0), s>>>(pb, d_a, smem_tables);
+    setup_kernel<<<pb.n, 128, base + (smem_tables ? tables : 0), s>>>(pb, d_a, smem_tables);
     SPB_CUDA_TRY(cudaGetLastError());
     return SPB_OK;
 }

@@ -191,7 +191,15 @@ __global__ void __launch_bounds__(32) pick_list_bin(Problem pb)
     const int lane = threadIdx.x;
     const unsigned full = 0xffffffffu;
     __shared__ unsigned s_pc[kHistPadded];
-    for (int b = lane; b < kHistBins; b += 32) s_pc[hist_pad_index(b)] = pb.pre_cnt[b];
+    {
+        // all of a lane's loads issued before the first store (one L2
+        // latency, not kPer of them in a row)
+        unsigned v[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) v[i] = __ldcg(pb.pre_cnt + lane + 32 * i);
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) s_pc[hist_pad_index(lane + 32 * i)] = v[i];
+    }
     __syncwarp();
     unsigned long long cn[kPer], cl = 0;
 #pragma unroll
@@ -231,9 +239,22 @@ __global__ void __launch_bounds__(32) dd_threshold(Problem pb)
     // place, each lane's 16 consecutive bins cost one L2 request per bin)
     __shared__ double s_h2[kHistPadded];
     __shared__ unsigned long long s_hc[kHistPadded];
-    for (int b = lane; b < kHistBins; b += 32) {
-        s_h2[hist_pad_index(b)] = __ldcg(pb.hist_s2 + b);
-        s_hc[hist_pad_index(b)] = __ldcg(pb.hist_cnt + b);
+    {
+        // all of a lane's loads issued before the first store (one L2
+        // latency, not 16 of them in a row)
+        constexpr int kPer = kHistBins / 32;
+        double v2[kPer];
+        unsigned long long vc[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            v2[i] = __ldcg(pb.hist_s2 + lane + 32 * i);
+            vc[i] = __ldcg(pb.hist_cnt + lane + 32 * i);
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            s_h2[hist_pad_index(lane + 32 * i)] = v2[i];
+            s_hc[hist_pad_index(lane + 32 * i)] = vc[i];
+        }
     }
     __syncwarp();
     const double mag = pb.comps == 1 ? fabs(rb->res[0].hi) : hypot(rb->res[0].hi, rb->res[1].hi);
@@ -284,61 +305,86 @@ __device__ __forceinline__ void stage(double* dst, const double* __restrict__ sr
 // Copies `parts` subset-sum tables laid out [q][n][G] (the walks' grouping,
 // q = d / G) into shared memory as [n][terms] (d contiguous per row), so
 // that lanes taking consecutive terms of one row read consecutive words
-// rather than words n*G apart in one bank.  A group of G words is
-// contiguous on both sides, so each thread moves whole groups (one index
-// division per group, not four per word), eight groups in flight.
+// rather than words n*G apart in one bank.  For even G the threads move
+// 16-byte pairs in destination order: consecutive lanes write consecutive
+// pairs of one row (no bank conflicts; the transposed order put a warp's
+// stores 8*terms bytes apart, all in one bank) and read half of one 32-byte
+// group each, eight pairs in flight per thread.
 __device__ __forceinline__ void stage_rows(double* dst, const double* __restrict__ src, int parts, int n,
                                            int terms, int G)
 {
-    const int per = terms * n, nq = terms / G, groups = parts * nq * n, bd = blockDim.x;
-    for (int j0 = threadIdx.x; j0 < groups; j0 += 8 * bd) {
-        double v[8][4];
+    const int per = terms * n, bd = blockDim.x;
+    if (G == 1) {  // n < 3: tiny tables
+        for (int i = threadIdx.x; i < parts * per; i += bd) {
+            const int part = i / per, rd = i % per, r = rd / terms, d = rd % terms;
+            dst[i] = src[(size_t)part * per + (size_t)d * n + r];
+        }
+        return;
+    }
+    const int half = terms / 2, total = parts * n * half, ppg = G / 2;  // pairs per row, all, per group
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    for (int t0 = threadIdx.x; t0 < total; t0 += 8 * bd) {
+        double2 v[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int j = j0 + k * bd;
-#pragma unroll
-            for (int g = 0; g < 4; ++g) v[k][g] = (j < groups && g < G) ? __ldg(src + (size_t)j * G + g) : 0.0;
+            const int t = t0 + k * bd;
+            if (t < total) {
+                // t = (part * n + r) * half + c, c = q * ppg + h
+                const int pr = t / half, c = t % half, part = pr / n, r = pr % n, q = c / ppg, h = c % ppg;
+                v[k] = __ldg(s2 + ((size_t)part * per + ((size_t)q * n + r) * G) / 2 + h);
+            }
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int j = j0 + k * bd;
-            if (j < groups) {
-                // j = (part * nq + q) * n + r
-                const int qr = j % (nq * n), part = j / (nq * n), q = qr / n, r = qr % n;
-                double* d = dst + (size_t)part * per + (size_t)r * terms + q * G;
-#pragma unroll
-                for (int g = 0; g < 4; ++g)
-                    if (g < G) d[g] = v[k][g];
-            }
+            const int t = t0 + k * bd;
+            if (t < total) d2[t] = v[k];
         }
     }
 }
 
-// Sums a dd over a worker: a warp, or the whole CTA (warp sums in warp
-// order through s_red).  The result is valid in the worker's thread 0.
-__device__ __forceinline__ dd worker_sum_dd(dd v, bool wide, dd* s_red)
+// Threads per refinement worker: a warp, doubled while every unit still
+// gets its own worker in one round over the grid's warps and each thread
+// keeps at least `per_lane` terms (two independent chains in the real
+// kernel, one in the complex).  Few units then spread over many warps
+// instead of leaving most of the grid idle behind a few long chains.
+__device__ __forceinline__ int refine_worker_threads(unsigned long long count, int terms, int per_lane)
+{
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+    int wk = 32;
+    while (2 * wk <= (int)blockDim.x && 2 * wk * per_lane <= terms && count * (unsigned long long)(2 * wk / 32) <= warps)
+        wk *= 2;
+    return wk;
+}
+
+// Sums a dd over a worker of wk threads (warp sums added in warp order
+// through s_red).  The result is valid in the worker's thread 0.  Every
+// thread of the CTA calls it when wk > 32 (it holds a block barrier).
+__device__ __forceinline__ dd worker_sum_dd(dd v, int wk, dd* s_red)
 {
     v = warp_sum_dd(v);
-    if (!wide) return v;
+    if (wk == 32) return v;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) s_red[wid] = v;
     __syncthreads();
-    if (threadIdx.x == 0)
-        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) v = dd_add(v, s_red[i]);
+    if (threadIdx.x % wk == 0)
+        for (int i = 1; i < wk / 32; ++i) v = dd_add(v, s_red[wid + i]);
     return v;
 }
 
-__device__ __forceinline__ void worker_sync(bool wide)
+__device__ __forceinline__ void worker_sync(int wk)
 {
-    if (wide) __syncthreads();
+    if (wk > 32) __syncthreads();
     else __syncwarp();
 }
 
-// A unit is refined by a worker: one warp per unit, or, when there are at
-// most as many units as CTAs, one CTA per unit (the units then spread over
-// more SMs).  Units are dealt out CTA by CTA (unit e to CTA e mod grid), so
-// that a few hundred units occupy every SM rather than filling a few.  A worker's threads take terms; each runs two independent term
-// chains at a time when it has two.
+// A unit is refined by a worker of wk threads (refine_worker_threads).
+// Units are dealt out CTA by CTA (unit e to CTA e mod grid), so that a few
+// hundred units occupy every SM rather than filling a few.  The loop runs in
+// rounds of one unit per worker, the same number of rounds in every CTA, so
+// that the block barriers of multi-warp workers are met by all threads.  A
+// worker's threads take terms; each runs two independent term chains at a
+// time when it has two.
 __global__ void __launch_bounds__(512) refine_real(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
@@ -347,8 +393,7 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
     __shared__ dd s_red[16];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
     const int nwarps = blockDim.x >> 5;
-    const bool wide = count <= (unsigned long long)gridDim.x;  // one unit per CTA at most
-    const int wk = wide ? blockDim.x : 32;               // threads per worker
+    const int wk = refine_worker_threads(count, terms, 2);  // threads per worker
     const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
     const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
     double* s_dh = sm;
@@ -366,51 +411,57 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
     double* xw = s_x + wid * 2 * n;
     double* gw = s_g + wid * nq;
     dd corr = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)wid * gridDim.x + blockIdx.x; e < count;
-         e += (unsigned long long)gridDim.x * nwk) {
-        if (pb.list_x) {
-            const double* src = pb.list_x + e * (2 * n);
-            for (int i = wl; i < 2 * n; i += wk) xw[i] = src[i];
-        } else {
-            unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
+    const unsigned long long round = (unsigned long long)gridDim.x * nwk;
+    for (unsigned long long e0 = 0; e0 < count; e0 += round) {
+        const unsigned long long e = e0 + (unsigned long long)wid * gridDim.x + blockIdx.x;
+        const bool active = e < count;
+        if (active) {
+            if (pb.list_x) {
+                const double* src = pb.list_x + e * (2 * n);
+                for (int i = wl; i < 2 * n; i += wk) xw[i] = src[i];
+            } else {
+                unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
+            }
         }
-        worker_sync(wide);
-        for (int q = wl; q < nq; q += wk) gw[q] = group_sum_real_rt(xw, s_dh + q * G, n, pb.na, G, terms);
+        worker_sync(wk);
         dd acc = {0.0, 0.0};
-        if (terms >= 2 * wk) {
-            for (int d = wl; d < terms; d += 2 * wk) {
-                const int d2 = d + wk;
-                dd p1 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
-                dd p2 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
-                for (int r = 1; r < n; ++r) {
-                    const int k1 = r * terms + d, k2 = r * terms + d2;
-                    const dd x = {xw[r], xw[n + r]};
-                    p1 = dd_mul(p1, dd_add_fast(x, dd{s_dh[k1], s_dl[k1]}));
-                    p2 = dd_mul(p2, dd_add_fast(x, dd{s_dh[k2], s_dl[k2]}));
+        if (active) {
+            for (int q = wl; q < nq; q += wk) gw[q] = group_sum_real_rt(xw, s_dh + q * G, n, pb.na, G, terms);
+            if (terms >= 2 * wk) {
+                for (int d = wl; d < terms; d += 2 * wk) {
+                    const int d2 = d + wk;
+                    dd p1 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
+                    dd p2 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
+                    for (int r = 1; r < n; ++r) {
+                        const int k1 = r * terms + d, k2 = r * terms + d2;
+                        const dd x = {xw[r], xw[n + r]};
+                        p1 = dd_mul(p1, dd_add_fast(x, dd{s_dh[k1], s_dl[k1]}));
+                        p2 = dd_mul(p2, dd_add_fast(x, dd{s_dh[k2], s_dl[k2]}));
+                    }
+                    acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p1)) : dd_add(acc, p1);
+                    acc = (__popc(d2) & 1) ? dd_add(acc, dd_neg(p2)) : dd_add(acc, p2);
                 }
-                acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p1)) : dd_add(acc, p1);
-                acc = (__popc(d2) & 1) ? dd_add(acc, dd_neg(p2)) : dd_add(acc, p2);
-            }
-        } else {
-            for (int d = wl; d < terms; d += wk) {
-                dd p = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
-                for (int r = 1; r < n; ++r) {
-                    const int k = r * terms + d;
-                    p = dd_mul(p, dd_add_fast(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
+            } else {
+                for (int d = wl; d < terms; d += wk) {
+                    dd p = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
+                    for (int r = 1; r < n; ++r) {
+                        const int k = r * terms + d;
+                        p = dd_mul(p, dd_add_fast(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
+                    }
+                    acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
                 }
-                acc = (__popc(d) & 1) ? dd_add(acc, dd_neg(p)) : dd_add(acc, p);
             }
         }
-        acc = worker_sum_dd(acc, wide, s_red);
-        worker_sync(wide);
-        if (wl == 0) {
+        acc = worker_sum_dd(acc, wk, s_red);
+        worker_sync(wk);
+        if (active && wl == 0) {
             double f = 0.0;
             for (int q = 0; q < nq; ++q) f = (__popc(q) & 1) ? sub_rn(f, gw[q]) : add_rn(f, gw[q]);
             dd c = dd_add_d(acc, -f);
             if (pb.list_u[e] & 1ull) c = dd_neg(c);
             corr = dd_add(corr, c);
         }
-        worker_sync(wide);
+        worker_sync(wk);
     }
     dd tot[1] = {corr};
     grid_reduce<1>(tot, pb);
@@ -424,8 +475,7 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
     __shared__ dd s_red[2][16];
     const int n = pb.n, G = pb.g, terms = 1 << pb.w, nq = terms / G;
     const int nwarps = blockDim.x >> 5;
-    const bool wide = count <= (unsigned long long)gridDim.x;  // one unit per CTA at most
-    const int wk = wide ? blockDim.x : 32;               // threads per worker
+    const int wk = refine_worker_threads(count, terms, 1);  // threads per worker
     const int wl = threadIdx.x % wk, wid = threadIdx.x / wk, nwk = blockDim.x / wk;
     const int ntp = n - 1 - pb.w > 0 ? n - 1 - pb.w : 0;
     double* s_dh = sm;                    // [2][terms*n]
@@ -447,47 +497,53 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
     double* xw = s_x + wid * 4 * n;  // xr hi, xr lo, xi hi, xi lo
     double* gw = s_g + wid * 2 * nq;
     dd corr_r = {0.0, 0.0}, corr_i = {0.0, 0.0};
-    for (unsigned long long e = (unsigned long long)wid * gridDim.x + blockIdx.x; e < count;
-         e += (unsigned long long)gridDim.x * nwk) {
-        if (pb.list_x) {
-            const double* src = pb.list_x + e * (4 * n);
-            for (int i = wl; i < 4 * n; i += wk) xw[i] = src[i];
-        } else {
-            unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
-            unit_base(pb, s_mt, pb.list_u[e], 1, wl, xw + 2 * n, xw + 3 * n, wk);
-        }
-        worker_sync(wide);
-        for (int q = wl; q < nq; q += wk)
-            group_sum_complex_rt(xw, xw + 2 * n, drh + q * G, dih + q * G, n, G, terms, gw[2 * q],
-                                 gw[2 * q + 1]);
-        dd ar = {0.0, 0.0}, ai = {0.0, 0.0};
-        for (int d = wl; d < terms; d += wk) {
-            int k = d;
-            dd pr = dd_add_fast(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
-            dd pi = dd_add_fast(dd{xw[2 * n], xw[3 * n]}, dd{dih[k], dil[k]});
-            for (int r = 1; r < n; ++r) {
-                k = r * terms + d;
-                dd yr = dd_add_fast(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
-                dd yi = dd_add_fast(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
-                // the products' sums unnormalised (dd_add_fast: about 2^-106 of
-                // |pr yr| + |pi yi| off, far inside what the refinement corrects)
-                dd nr = dd_add_fast(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
-                dd ni = dd_add_fast(dd_mul(pr, yi), dd_mul(pi, yr));
-                pr = nr;
-                pi = ni;
-            }
-            if (__popc(d) & 1) {
-                ar = dd_add(ar, dd_neg(pr));
-                ai = dd_add(ai, dd_neg(pi));
+    const unsigned long long round = (unsigned long long)gridDim.x * nwk;
+    for (unsigned long long e0 = 0; e0 < count; e0 += round) {
+        const unsigned long long e = e0 + (unsigned long long)wid * gridDim.x + blockIdx.x;
+        const bool active = e < count;
+        if (active) {
+            if (pb.list_x) {
+                const double* src = pb.list_x + e * (4 * n);
+                for (int i = wl; i < 4 * n; i += wk) xw[i] = src[i];
             } else {
-                ar = dd_add(ar, pr);
-                ai = dd_add(ai, pi);
+                unit_base(pb, s_mt, pb.list_u[e], 0, wl, xw, xw + n, wk);
+                unit_base(pb, s_mt, pb.list_u[e], 1, wl, xw + 2 * n, xw + 3 * n, wk);
             }
         }
-        ar = worker_sum_dd(ar, wide, s_red[0]);
-        ai = worker_sum_dd(ai, wide, s_red[1]);
-        worker_sync(wide);
-        if (wl == 0) {
+        worker_sync(wk);
+        dd ar = {0.0, 0.0}, ai = {0.0, 0.0};
+        if (active) {
+            for (int q = wl; q < nq; q += wk)
+                group_sum_complex_rt(xw, xw + 2 * n, drh + q * G, dih + q * G, n, G, terms, gw[2 * q],
+                                     gw[2 * q + 1]);
+            for (int d = wl; d < terms; d += wk) {
+                int k = d;
+                dd pr = dd_add_fast(dd{xw[0], xw[n]}, dd{drh[k], drl[k]});
+                dd pi = dd_add_fast(dd{xw[2 * n], xw[3 * n]}, dd{dih[k], dil[k]});
+                for (int r = 1; r < n; ++r) {
+                    k = r * terms + d;
+                    dd yr = dd_add_fast(dd{xw[r], xw[n + r]}, dd{drh[k], drl[k]});
+                    dd yi = dd_add_fast(dd{xw[2 * n + r], xw[3 * n + r]}, dd{dih[k], dil[k]});
+                    // the products' sums unnormalised (dd_add_fast: about 2^-106 of
+                    // |pr yr| + |pi yi| off, far inside what the refinement corrects)
+                    dd nr = dd_add_fast(dd_mul(pr, yr), dd_neg(dd_mul(pi, yi)));
+                    dd ni = dd_add_fast(dd_mul(pr, yi), dd_mul(pi, yr));
+                    pr = nr;
+                    pi = ni;
+                }
+                if (__popc(d) & 1) {
+                    ar = dd_add(ar, dd_neg(pr));
+                    ai = dd_add(ai, dd_neg(pi));
+                } else {
+                    ar = dd_add(ar, pr);
+                    ai = dd_add(ai, pi);
+                }
+            }
+        }
+        ar = worker_sum_dd(ar, wk, s_red[0]);
+        ai = worker_sum_dd(ai, wk, s_red[1]);
+        worker_sync(wk);
+        if (active && wl == 0) {
             double fr = 0.0, fi = 0.0;
             for (int q = 0; q < nq; ++q) {
                 if (__popc(q) & 1) {
@@ -506,7 +562,7 @@ __global__ void __launch_bounds__(512) refine_complex(Problem pb)
             corr_r = dd_add(corr_r, cr);
             corr_i = dd_add(corr_i, ci);
         }
-        worker_sync(wide);
+        worker_sync(wk);
     }
     dd tot[2] = {corr_r, corr_i};
     grid_reduce<2>(tot, pb);
