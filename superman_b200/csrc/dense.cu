@@ -460,6 +460,16 @@ int run(const double* a, bool a_on_device, int n, int comps, const spb_options* 
     pb.threads = threads;
     const bool dd_mode = opt.precision == SPB_PREC_DD;
     pb.mode = dd_mode ? 1 : 0;
+    if (dd_mode && pb.na == n) {
+        // the refinement stages both table words of every part (256 threads
+        // at the least): refuse before any launch when they cannot fit
+        const size_t rs = refine_smem_bytes(pb, 256);
+        if (rs + 2048 > ctx->smem_optin) {
+            spb_set_error("dense n=%d, unit_bits=%d: the double-double refinement needs %zu B shared memory "
+                          "(limit %zu B); use fewer unit bits", n, pb.w, rs, ctx->smem_optin);
+            return out->status = SPB_ERR_INVALID;
+        }
+    }
 
     size_t in_off = 0;
     size_t need = plan_layout(&pb, nullptr, &in_off);

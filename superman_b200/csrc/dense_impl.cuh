@@ -701,8 +701,9 @@ __global__ void __launch_bounds__(ComplexCfg<N>::kMaxThreads, 1) walk_complex(Pr
 //                      range, bases rebuilt from scratch;
 //   launch_refine      re-evaluates the listed units in double-double and
 //                      writes sum(double-double unit sum - the walk's FP64
-//                      unit sum) to rb->corr, one warp per unit; it refines
-//                      nothing unless rb->list_n == rb->count <= pb.list_cap.
+//                      unit sum) to rb->corr, a worker of one or more warps
+//                      per unit; it refines nothing unless
+//                      rb->list_n == rb->count <= pb.list_cap.
 // bound_walk + pick_list_bin run before the walk and set the bin from which
 // the walk lists its units.  A mode-2 walk (same launch shape as mode 1)
 // replays the listing with the walk's own bases (pb.list_x) when the host
@@ -711,6 +712,9 @@ int launch_threshold(const Problem& pb, cudaStream_t s);
 int launch_refine(const Problem& pb, int blocks, cudaStream_t s);
 int launch_bound_pass(const Problem& pb, int blocks, cudaStream_t s);
 int launch_listing(const Problem& pb, cudaStream_t s);
+// Dynamic shared memory of the refinement at `threads` threads per CTA: both
+// words of every part's table, per-warp bases and group sums, high columns.
+size_t refine_smem_bytes(const Problem& pb, int threads);
 
 // FP32-product walks (f32_impl.cuh), n <= kMaxF32N.  A result whose
 // estimated relative error exceeds opt.rel_tol (kF32DefaultBound when unset,

@@ -50,6 +50,46 @@ def test_dense_shape_invariance(spb, oracle, unit_bits, threads, blocks):
     assert oracle.rel_err(r.permanent, exact) <= REL_TOL_SMALL
 
 
+@pytest.mark.parametrize("small_call", [0, -1])
+@pytest.mark.parametrize("precision", ["fp64", "dd"])
+@pytest.mark.parametrize("unit_bits", [9, 10])
+def test_dense_wide_units(spb, oracle, unit_bits, precision, small_call):
+    # Tables of 2^9 and 2^10 entries per row: every level above 32 entries
+    # takes several passes of the setup kernel's per-row warp (small_call=-1
+    # keeps the separate kernels; 2^10 does not fit the fused call anyway).
+    a = W.dense_uniform(18, seed=6)
+    exact = oracle.exact_perm(a)
+    if precision == "dd" and unit_bits == 10:
+        # both table words of 2^10 x 18 entries (295 KB) exceed the
+        # refinement's shared memory: refused before any launch
+        with pytest.raises(spb.SupermanError) as e:
+            spb.perm_dense(a, precision=precision, unit_bits=unit_bits, small_call=small_call)
+        assert "use fewer unit bits" in str(e.value)
+        return
+    r = spb.perm_dense(a, precision=precision, unit_bits=unit_bits, small_call=small_call)
+    assert oracle.rel_err(r.permanent, exact) <= REL_TOL_SMALL
+
+
+@pytest.mark.parametrize("unit_bits", [7, 8])
+def test_complex_wide_units(spb, oracle, unit_bits):
+    # (2^9 would need 2 parts x 2 words x 2^9 x 16 doubles, 262 KB, in the
+    # refinement's shared memory: refused like the real case below)
+    a = W.haar_block(16, seed=91, N=64)
+    er, ei = oracle.exact_perm_complex(a)
+    r = spb.perm_complex(a, precision="dd", unit_bits=unit_bits)
+    scale = float(np.prod(np.abs(a).sum(axis=1)))
+    assert abs(r.permanent - complex(float(er), float(ei))) <= 1e-13 * scale
+
+
+def test_dense_unit_bits_too_wide(spb):
+    # 2^14 table entries per row do not fit the walk's shared memory: a clean
+    # error before any launch.
+    a = W.dense_uniform(18, seed=7)
+    with pytest.raises(spb.SupermanError) as e:
+        spb.perm_dense(a, unit_bits=14)
+    assert "shared memory" in str(e.value)
+
+
 def test_dense_known_answers(spb):
     # perm(c J_n) = n! c^n  (ExampleMatrices/dense.mtx is 0.91 J_45)
     import math
