@@ -12,7 +12,7 @@
 // only if either count disagrees with the histogram from a replay scan (walk mode 2,
 // same launch shape, so the unit bases are bit-identical) that lists them
 // with their double-double base vectors.  This kernel then re-evaluates each
-// listed unit, one warp per unit:
+// listed unit on a worker of one or more warps:
 //   * the FP64 unit sum exactly as the walk computed it (same operations in
 //     the same order, so the same bits), spread over the lanes by group;
 //   * the double-double unit sum (x_r = xtop_r + DE[d][r] in double-double,
