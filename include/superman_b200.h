@@ -72,7 +72,11 @@ typedef struct spb_options {
     int precision;         /* enum spb_precision                             */
     double rel_tol;        /* SPB_PREC_DD target relative error (0 = 1e-13);
                               SPB_PREC_FP32 accepted error (0 = 1e-12)      */
-    int unit_bits;         /* log2 Gray terms per unit; 0 = automatic        */
+    int unit_bits;         /* log2 Gray terms per unit; 0 = automatic.  A
+                              width whose tables do not fit shared memory
+                              (the walk's, or with SPB_PREC_DD both words
+                              of the refinement's) is refused with
+                              SPB_ERR_INVALID before any launch             */
     int threads_per_block; /* 0 = automatic                                  */
     int blocks;            /* 0 = automatic (persistent: one CTA per SM)     */
     void* stream;          /* cudaStream_t to run on; NULL = library stream  */
