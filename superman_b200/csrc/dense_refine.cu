@@ -321,7 +321,10 @@ __device__ __forceinline__ void stage_rows(double* dst, const double* __restrict
         }
         return;
     }
-    const int half = terms / 2, total = parts * n * half, ppg = G / 2;  // pairs per row, all, per group
+    // terms is a power of two and G is 2 or 4, so the index splits by shifts
+    // and masks; parts is 1 or 2 (no division by n either)
+    const int half = terms / 2, total = parts * n * half;  // pairs per row, all
+    const int lh = __ffs(half) - 1, lp = G == 4 ? 1 : 0;    // log2 half, log2 pairs per group
     const double2* s2 = reinterpret_cast<const double2*>(src);
     double2* d2 = reinterpret_cast<double2*>(dst);
     for (int t0 = threadIdx.x; t0 < total; t0 += 8 * bd) {
@@ -330,8 +333,9 @@ __device__ __forceinline__ void stage_rows(double* dst, const double* __restrict
         for (int k = 0; k < 8; ++k) {
             const int t = t0 + k * bd;
             if (t < total) {
-                // t = (part * n + r) * half + c, c = q * ppg + h
-                const int pr = t / half, c = t % half, part = pr / n, r = pr % n, q = c / ppg, h = c % ppg;
+                // t = (part * n + r) * half + c, c = q * (G / 2) + h
+                const int pr = t >> lh, c = t & (half - 1), part = pr >= n ? 1 : 0, r = pr - part * n;
+                const int q = c >> lp, h = c & lp;
                 v[k] = __ldg(s2 + ((size_t)part * per + ((size_t)q * n + r) * G) / 2 + h);
             }
         }
@@ -385,7 +389,7 @@ __device__ __forceinline__ void worker_sync(int wk)
 // that the block barriers of multi-warp workers are met by all threads.  A
 // worker's threads take terms; each runs two independent term chains at a
 // time when it has two.
-__global__ void __launch_bounds__(512) refine_real(Problem pb)
+__global__ void __launch_bounds__(512, 1) refine_real(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
     if (count == 0) return;
@@ -432,7 +436,25 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
                     const int d2 = d + wk;
                     dd p1 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
                     dd p2 = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d2], s_dl[d2]});
-                    for (int r = 1; r < n; ++r) {
+                    int r = 1;
+                    // four rows' factors formed ahead of the products (they
+                    // do not depend on them), then multiplied in row order
+                    for (; r + 3 < n; r += 4) {
+                        dd y1[4], y2[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int k1 = (r + k) * terms + d, k2 = (r + k) * terms + d2;
+                            const dd x = {xw[r + k], xw[n + r + k]};
+                            y1[k] = dd_add_fast(x, dd{s_dh[k1], s_dl[k1]});
+                            y2[k] = dd_add_fast(x, dd{s_dh[k2], s_dl[k2]});
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            p1 = dd_mul(p1, y1[k]);
+                            p2 = dd_mul(p2, y2[k]);
+                        }
+                    }
+                    for (; r < n; ++r) {
                         const int k1 = r * terms + d, k2 = r * terms + d2;
                         const dd x = {xw[r], xw[n + r]};
                         p1 = dd_mul(p1, dd_add_fast(x, dd{s_dh[k1], s_dl[k1]}));
@@ -444,7 +466,18 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
             } else {
                 for (int d = wl; d < terms; d += wk) {
                     dd p = dd_add_fast(dd{xw[0], xw[n]}, dd{s_dh[d], s_dl[d]});
-                    for (int r = 1; r < n; ++r) {
+                    int r = 1;
+                    for (; r + 3 < n; r += 4) {
+                        dd y[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int i = (r + k) * terms + d;
+                            y[k] = dd_add_fast(dd{xw[r + k], xw[n + r + k]}, dd{s_dh[i], s_dl[i]});
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) p = dd_mul(p, y[k]);
+                    }
+                    for (; r < n; ++r) {
                         const int k = r * terms + d;
                         p = dd_mul(p, dd_add_fast(dd{xw[r], xw[n + r]}, dd{s_dh[k], s_dl[k]}));
                     }
@@ -467,7 +500,7 @@ __global__ void __launch_bounds__(512) refine_real(Problem pb)
     grid_reduce<1>(tot, pb);
 }
 
-__global__ void __launch_bounds__(512) refine_complex(Problem pb)
+__global__ void __launch_bounds__(512, 1) refine_complex(Problem pb)
 {
     const unsigned long long count = refine_count(pb);
     if (count == 0) return;
