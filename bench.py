@@ -771,6 +771,21 @@ def other_arm(args, wl):
         got = d_out.cpu().numpy()[0::2]
         want0 = S.perm_dense(mats[0]).permanent
         assert abs(got[0] - want0) <= 1e-13 * abs(want0)
+        # end to end: the matrices from page-locked host memory to the device,
+        # the batched call, the results back, every step (host clock)
+        h_in = torch.from_numpy(mats).pin_memory()
+        h_out = torch.empty(count * 2, dtype=torch.float64).pin_memory()
+
+        def step_e2e():
+            d_in.copy_(h_in, non_blocking=True)
+            step()
+            h_out.copy_(d_out, non_blocking=True)
+            torch.cuda.synchronize()
+        step_e2e()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_e2e()
+        t_e2e = (time.perf_counter() - t0) / args.steps
         line = {"metric": "batched_perms_per_s", "value": count / t, "unit": "perms/s",
                 "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -780,6 +795,10 @@ def other_arm(args, wl):
                            "timing": "host clock around the launches, device-wide synchronize after"},
                 "roofline": {"bound": "fp64", "achieved": alg / t / 1e12, "peak": peak.value / 1e12,
                              "unit": "T FP64-pipe inst/s", "frac": alg / t / peak.value, "traffic": None},
+                "e2e": {"value": count / t_e2e, "unit": "perms/s", "h2d_bytes_per_step": int(mats.nbytes),
+                        "d2h_bytes_per_step": int(h_out.numel() * 8),
+                        "timing": "host clock per step: pinned host matrices copied in, spb_perm_batch_dev, "
+                                  "results copied back, synchronize"},
                 "clocks": clk.summary(), "gpu_launches": args.steps}
         print(json.dumps(line), flush=True)
         return 0
@@ -788,10 +807,18 @@ def other_arm(args, wl):
         samples = 1 << 22
         for _ in range(args.warmup):
             S.perm_approx(a, samples=1 << 16, seed=1)
+        rs, walls = [], []
         with ClockSampler(0) as clk:
-            rs = [S.perm_approx(a, samples=samples, seed=1 + k) for k in range(args.steps)]
+            for k in range(args.steps):
+                t0 = time.perf_counter()
+                rs.append(S.perm_approx(a, samples=samples, seed=1 + k))
+                walls.append(time.perf_counter() - t0)
         t = statistics.mean(x.kernel_s for x in rs)
         dt = statistics.mean(x.time for x in rs)
+        nnz = int(np.count_nonzero(a))
+        # the call copies the pattern (row and column pointers and indices)
+        # and the two float scaling vectors in, the two-double total out
+        h2d = 4 * 2 * (n + 1) + 4 * 2 * nnz + 4 * 2 * n
         line = {"metric": "samples_per_s", "value": samples / t, "unit": "samples/s",
                 "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
@@ -799,7 +826,11 @@ def other_arm(args, wl):
                 "config": {"workload": desc, "n": n, "samples": samples, "estimate": rs[0].permanent,
                            "rel_std_error": rs[0].err_est,
                            "timing": "kernel events of spb_perm_approx; samples per step = 2^22"},
-                "roofline": None, "clocks": clk.summary(), "gpu_launches": args.steps}
+                "roofline": None,
+                "e2e": {"value": samples / statistics.mean(walls), "unit": "samples/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": 16,
+                        "timing": "host clock around each perm_approx call on the host 0/1 matrix"},
+                "clocks": clk.summary(), "gpu_launches": args.steps}
         print(json.dumps(line), flush=True)
         return 0
     if kind == "binary":
@@ -807,11 +838,28 @@ def other_arm(args, wl):
         _lib.check(L.spb_measure_pipe_peak(0, 1, ctypes.byref(peak)))
         for _ in range(args.warmup):
             r = S.perm_binary(a)
+        rs, walls = [], []
         with ClockSampler(0) as clk:
-            rs = [S.perm_binary(a) for _ in range(args.steps)]
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                rs.append(S.perm_binary(a))
+                walls.append(time.perf_counter() - t0)
         assert all(x.permanent == rs[0].permanent for x in rs)
         t = statistics.mean(x.kernel_s for x in rs)
         dt = statistics.mean(x.time for x in rs)
+        # what the call copies: the start vector, the doubled low-column
+        # table and the high columns in (its width rule), the limbs out
+        wb = 8
+        while wb > 2 and ((1 << wb) * n * 4 > 32 * 1024 or n - 1 - wb < 16):
+            wb -= 1
+        h2d = 4 * n + 4 * (1 << wb) * n + (n - 1 - wb) * n
+        # limbs read back: the Bregman-Minc bound rule of the call
+        nz = a != 0
+        def side(m):
+            rs_ = m.sum(axis=1)
+            return sum(math.lgamma(r + 1) / math.log(2) / r for r in rs_) if rs_.min() > 0 else 0.0
+        bits = min(side(nz), side(nz.T)) + (n - 1) + 2
+        limbs = 4 if bits <= 128 else 5 if bits <= 160 else 6 if bits <= 192 else 10 if bits <= 320 else 12
         steps = n * 2 ** (n - 1)  # the integer NW walk: 2^(n-1) subsets of n rows
         alg = 2 * steps  # one integer add + one multiply per row per subset
         line = {"metric": "ryser_gray_steps_per_s", "value": steps / t, "unit": "gray-steps/s (NW, n*2^(n-1))",
@@ -823,6 +871,9 @@ def other_arm(args, wl):
                 "roofline": {"bound": "int", "achieved": alg / t / 1e12, "peak": peak.value / 1e12,
                              "unit": "T int32 ops/s (add+mul per row-update) vs IMAD pipe",
                              "frac": alg / t / peak.value, "traffic": None},
+                "e2e": {"value": steps / statistics.mean(walls), "unit": "gray-steps/s (NW, n*2^(n-1))",
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 * limbs,
+                        "timing": "host clock around each perm_binary call on the host 0/1 matrix"},
                 "clocks": clk.summary(), "gpu_launches": args.steps}
     else:
         a = W.sparse_perm_plus(n, seed)
