@@ -81,6 +81,24 @@ def test_complex_conjugation_n24(spb):
     assert abs(r2.permanent - np.conj(r1.permanent)) <= 1e-13 * abs(r1.permanent)
 
 
+def test_complex_two_term_groups_n34(spb):
+    """n = 34 complex runs the two-term groups (n > 32).  perm(A^T) = perm(A);
+    a row times i gives i perm(A) (exact in the input); a row times 2 gives
+    exactly twice the result (rows are pre-scaled by powers of two, so the
+    walk sees the same matrix)."""
+    a = W.haar_block(34, 21)
+    r1 = spb.perm_complex(a, precision="dd").permanent
+    r2 = spb.perm_complex(np.ascontiguousarray(a.T), precision="dd").permanent
+    assert abs(r2 - r1) <= 1e-11 * abs(r1)
+    b = a.copy()
+    b[5] *= 1j
+    r3 = spb.perm_complex(b, precision="dd").permanent
+    assert abs(r3 - 1j * r1) <= 1e-11 * abs(r1)
+    b = a.copy()
+    b[9] *= 2.0
+    assert spb.perm_complex(b, precision="dd").permanent == 2.0 * r1
+
+
 def test_injected_allocation_failure_and_recovery(spb):
     L = _lib.lib()
     a = W.dense_uniform(20, 16)
