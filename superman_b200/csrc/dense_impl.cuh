@@ -71,13 +71,16 @@ struct Problem {
     unsigned short* raw_b;         // [raw_cap] its bound bin
 };
 
-// Capacity of the mode-1 list (units).  pick_list_bin aims at kRawTarget,
-// an eighth of it, so that bins computed by the walk and by bound_walk may
-// differ at bin edges; the units the refinement takes (a few hundred to a
-// few thousand from n = 27 to 32) fit that target many times over, and every
-// listed unit costs the walk an append.
-constexpr unsigned long long kRawCap = 1ull << 17;
-constexpr unsigned long long kRawTarget = kRawCap / 8;
+// Capacity of the mode-1 list (units; 10 bytes each, 21 MB).  A walk of at
+// most kRawCap / 2 units (real n <= 29, complex n <= 28 at the default unit
+// width) lists every unit and needs no bound pass; larger walks list from
+// the bin pick_list_bin chooses, aiming at kRawTarget units, far below the
+// capacity so that bins computed by the walk and by bound_walk may differ at
+// bin edges.  The units the refinement takes (a few hundred to a few thousand
+// from n = 27 to 32) fit that target many times over, and every listed unit
+// costs the walk an append.
+constexpr unsigned long long kRawCap = 1ull << 21;
+constexpr unsigned long long kRawTarget = 1ull << 14;
 
 // Appends unit u (bound bin b) to the mode-1 list when b >= lbin.  The
 // appending lanes of a warp take their slots with one atomic (a leader
